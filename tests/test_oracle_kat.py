@@ -1,0 +1,163 @@
+"""Pins the oracle against the reference's own docked outputs.
+
+The reference writes, for every docking mode, `REMARK VINA RESULT: e lb ub`
+(main.cpp:159-170): the final adjusted score (model.cpp:1428-1431, printed
+with one decimal) and the RMSD lower/upper bounds to mode 1 (model.cpp:
+1485-1523, three decimals).  Rescoring the written coordinates with the
+oracle must reproduce them.  Tolerances: energy 0.08 kcal/mol (0.05 print
+rounding plus the 3-decimal coordinate rounding of the PDBQT writer), RMSD
+0.0015 A (0.0005 print rounding plus coordinate rounding).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+
+def load(golden_dir):
+    return np.load(os.path.join(golden_dir, "kat_vina.npz"))
+
+
+def ligand(z, key):
+    d = {k: z[f"{key}_{k}"] for k in ("xs", "el", "atom_node", "node_parent",
+                                      "node_origin_atom", "node_axis_atom", "pairs")}
+    d["num_tors"] = float(z[f"{key}_num_tors"])
+    models = z[f"{key}_models"]
+    d["xyz"] = models[0]
+    d["n_atoms"] = models.shape[1]
+    return d, models, z[f"{key}_remarks"]
+
+
+def test_known_answers_all_modes(golden_dir):
+    z = load(golden_dir)
+    names = list(z["names"])
+    assert len(names) >= 30
+    worst_e = worst_r = 0.0
+    for i, name in enumerate(names):
+        o = O.Oracle()
+        o.set_receptor(z["rec_xyz"], z["rec_xs"])
+        o.set_box(z["center"], z["size"])
+        d, models, remarks = ligand(z, f"L{i}")
+        lid = o.add_ligand(d)
+        intra_best = o.intramolecular_coords(lid, models[0])
+        for m, (e_ref, lb_ref, ub_ref) in zip(models, remarks):
+            e = o.eval_adjusted_coords(lid, m, intra_best)
+            lb, ub = o.rmsd(lid, m, models[0])
+            worst_e = max(worst_e, abs(e - e_ref))
+            worst_r = max(worst_r, abs(lb - lb_ref), abs(ub - ub_ref))
+            assert abs(e - e_ref) <= 0.08, (name, e, e_ref)
+            assert abs(lb - lb_ref) <= 0.0015 and abs(ub - ub_ref) <= 0.0015, (name, lb, ub, lb_ref, ub_ref)
+    print(f"worst |de|={worst_e:.3f} worst |drmsd|={worst_r:.4f}")
+
+
+def test_parser_reproduces_fixture_topology(golden_dir):
+    import gzip
+    import pdbqt_oracle as P
+    z = load(golden_dir)
+    text = gzip.open(os.path.join(golden_dir, "pdbqt", "1u1b_docking_result.pdbqt.gz"), "rt").read()
+    models = P.split_models(text)
+    lig = P.parse_ligand(models[0][1]).descriptor()
+    d, m, _ = ligand(z, "L0")
+    for k in ("xs", "atom_node", "node_parent", "pairs"):
+        np.testing.assert_array_equal(lig[k], d[k])
+    assert lig["num_tors"] == d["num_tors"] == 15.0
+
+
+def test_receptor_typing_matches_fixture(golden_dir):
+    import gzip
+    import pdbqt_oracle as P
+    z = load(golden_dir)
+    xyz, xs = P.parse_receptor(gzip.open(os.path.join(golden_dir, "pdbqt", "1u1b_protein.pdbqt.gz"), "rt").read())
+    np.testing.assert_array_equal(xs, z["rec_xs"])
+    np.testing.assert_array_equal(xyz, z["rec_xyz"])
+
+
+def test_lut_structure():
+    """precalculate.h:121-140: fast[i] = (smooth[i]+smooth[i+1])/2, dor by
+    central difference, zero at both ends."""
+    o = O.Oracle()
+    fast, se, sd = o.tables()
+    np.testing.assert_allclose(fast[:, :-1], 0.5 * (se[:, :-1] + se[:, 1:]), rtol=0, atol=0)
+    assert np.all(sd[:, 0] == 0) and np.all(sd[:, -1] == 0)
+    rs = np.sqrt(np.arange(2051) / 32.0)
+    dor = (se[:, 2:] - se[:, :-2]) / ((rs[2:] - rs[:-2]) * rs[1:-1])
+    np.testing.assert_allclose(sd[:, 1:-1], dor, rtol=1e-12, atol=1e-12)
+
+
+def test_analytic_gradient_matches_central_difference(golden_dir):
+    """Oracle's tree adjoint (tree.h:373-422) against central differences of
+    its own energy for the 1u1b ligand on the cached grid.
+
+    The reference's energy is only piecewise smooth: intra pairs jump at the
+    8 A cutoff (the gauss2 term is not zero there, weighted_terms.cpp:64 does
+    not test the cutoff) and trilinear interpolation has gradient kinks at
+    cell faces.  A central difference with h = 1e-4 that straddles one is
+    wrong by design, so a component passes when the FD at h = 1e-4, 1e-5 or
+    1e-6 agrees within 1e-3 * max(1, |g|_inf); at least 90% of components
+    must already agree at h = 1e-4."""
+    z = load(golden_dir)
+    o = O.Oracle()
+    o.set_receptor(z["rec_xyz"], z["rec_xs"])
+    o.set_box(z["center"], z["size"])
+    d, models, _ = ligand(z, "L0")
+    lid = o.add_ligand(d)
+    o.build_grids(sorted(set(int(t) for t in d["xs"] if t >= 0)))
+    nt = o.ntors[lid]
+    rng = np.random.default_rng(0)
+    n_ok_1e4 = n_tot = 0
+    for trial in range(3):
+        conf = np.zeros(7 + nt)
+        conf[:3] = d["xyz"][d["node_origin_atom"][0]] + rng.uniform(-0.5, 0.5, 3)
+        conf[3:7] = quat_increment(np.array([1.0, 0, 0, 0]), rng.uniform(-0.2, 0.2, 3))
+        conf[7:] = rng.uniform(-0.3, 0.3, nt)
+        e, g = o.eval_deriv(lid, conf, v=(1000, 1000, 1000), slope=1e6)
+        tol = 1e-3 * max(1.0, np.abs(g).max())
+        fds = [fd_grad(o, lid, conf, nt, h) for h in (1e-4, 1e-5, 1e-6)]
+        err = np.min(np.abs(np.stack(fds) - g), axis=0)
+        assert np.all(err <= tol), (trial, err.max(), tol)
+        n_ok_1e4 += int(np.sum(np.abs(fds[0] - g) <= tol))
+        n_tot += len(g)
+    assert n_ok_1e4 >= 0.9 * n_tot
+
+
+def fd_grad(o, lid, conf, nt, h):
+    fd = np.zeros(6 + nt)
+    for k in range(6 + nt):
+        def shifted(s):
+            c = conf.copy()
+            if k < 3:
+                c[k] += s
+            elif k < 6:
+                rot = np.zeros(3)
+                rot[k - 3] = s
+                c[3:7] = quat_increment(c[3:7], rot)
+            else:
+                c[7 + k - 6] += s
+            return o.eval_deriv(lid, c, v=(1000, 1000, 1000), slope=1e6)[0]
+        fd[k] = (shifted(h) - shifted(-h)) / (2 * h)
+    return fd
+
+
+def quat_increment(q, rot):
+    ang = np.linalg.norm(rot)
+    if ang < 1e-300:
+        return q
+    ax = rot / ang
+    a = np.array([np.cos(ang / 2), *(np.sin(ang / 2) * ax)])
+    w1, x1, y1, z1 = a
+    w2, x2, y2, z2 = q
+    out = np.array([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2,
+                    w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                    w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2,
+                    w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2])
+    return out / np.linalg.norm(out)
+
+
+def test_philox_known_answer():
+    """Philox4x32-10 known-answer vectors of the Random123 distribution."""
+    assert O.philox([0, 0, 0, 0], [0, 0]) == [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]
+    assert O.philox([0xffffffff] * 4, [0xffffffff] * 2) == [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]
+    assert O.philox([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344],
+                    [0xa4093822, 0x299f31d0]) == [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]
