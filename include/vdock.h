@@ -1,0 +1,201 @@
+/*
+ * vdock -- B200-native Vina-style docking hot path, C ABI.
+ *
+ * Replaces the two host entry points of HPCLab-933/Vina-CUDA
+ * (Vina-CUDA_v1.1):
+ *   kernel_grid  (inc/cuda/kernel1.cuh:30-40, def kernel1.cu:202)  -> vd_build_grids
+ *   kernel_monte (inc/cuda/kernel2.cuh:25-37, def kernel2.cu:566)  -> vd_dock / vd_dock_plain
+ * and the host packing around them in lib/main_procedure_cu.cpp:131-1006.
+ *
+ * Conventions (all entry points):
+ *   - plain C types only; host pointers unless a name ends in _device;
+ *   - every call returns vd_status; vd_last_error() gives a message for the
+ *     calling thread's last failure;
+ *   - a context owns one CUDA device, its stream and all device buffers;
+ *     calls on one context must not run concurrently (thread-compatible,
+ *     not thread-safe per context);
+ *   - calls are synchronous with respect to the host buffers they take.
+ *
+ * Pose layout ("conf", cf. output_type_cl, inc/kernel2.h:118-127):
+ *   position[3], quaternion[4] (w,x,y,z), torsions[ntors]    stride 7+ntors
+ * Gradient layout (cf. change_cl, inc/kernel2.h:129-136):
+ *   force[3], torque[3], d/dtorsion[ntors]                    stride 6+ntors
+ */
+#ifndef VDOCK_H
+#define VDOCK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    VD_OK = 0,
+    VD_ERR_CUDA = 1,      /* a CUDA runtime call failed                        */
+    VD_ERR_CAPACITY = 2,  /* input exceeds a compiled limit (atoms, torsions)  */
+    VD_ERR_ARG = 3,       /* invalid argument or call order                    */
+    VD_ERR_TIMEOUT = 4,   /* a device loop hit its iteration budget            */
+    VD_ERR_PARSE = 5,     /* malformed PDBQT / config input                    */
+    VD_ERR_NOMEM = 6      /* allocation failed or the context memory cap hit   */
+} vd_status;
+
+#define VD_MAX_ATOMS 128      /* heavy atoms per ligand (inc/kernel2.h:36)      */
+#define VD_MAX_TORS 48        /* torsions per ligand   (inc/kernel2.h:37)       */
+#define VD_MAX_PAIRS 4096     /* intra-ligand pairs (reference: 2048)           */
+#define VD_MAX_MODES 20       /* poses kept per ligand (main.cpp:394)           */
+#define VD_XS_TYPES 17
+
+typedef struct vd_ctx vd_ctx;
+
+/* Ligand topology.  Atoms are grouped contiguously by rigid body and rigid
+ * bodies are numbered in depth-first pre-order (body k>0 carries torsion k-1),
+ * the order lib/parse_pdbqt.cpp:342-401 produces.  Atoms with xs < 0
+ * (hydrogens) move with their body but carry no energy. */
+typedef struct {
+    int32_t n_atoms, n_nodes, n_pairs;
+    const double*  xyz;              /* [n_atoms*3] input conformation             */
+    const int32_t* xs;               /* [n_atoms] XS type 0..16 or -1              */
+    const int32_t* el;               /* [n_atoms] element (0 = H)                  */
+    const int32_t* atom_node;        /* [n_atoms] rigid body of each atom          */
+    const int32_t* node_parent;      /* [n_nodes] parent body, -1 for the root     */
+    const int32_t* node_origin_atom; /* [n_nodes] atom at the body's origin        */
+    const int32_t* node_axis_atom;   /* [n_nodes] parent-side atom of the rotatable
+                                        bond, -1 for the root                      */
+    const int32_t* pairs;            /* [n_pairs*2] intra pairs (model.cpp:875-900) */
+    double num_tors;                 /* N_tors of terms.cpp:97-128                 */
+} vd_ligand_desc;
+
+typedef struct {
+    double v_intra;   /* curl cap of intra pairs  (v[0], model.cpp:1330)       */
+    double v_inter;   /* curl cap of grid term    (v[1])                       */
+    double slope;     /* out-of-box penalty slope (main.cpp:400: 1e6)          */
+} vd_eval_params;
+
+typedef struct {
+    uint32_t seed;
+    int32_t  n_chains;        /* MC chains per ligand (--thread)               */
+    int32_t  search_depth;    /* MC steps per chain; 0 = main.cpp:354-391 rule,
+                                 < 0 = none (chains return their initial pose) */
+    int32_t  max_bfgs_steps;  /* 0 = (30 + atoms)/3 (main.cpp:386)             */
+    int32_t  num_modes;       /* modes returned (<= VD_MAX_MODES)              */
+    double   energy_range;    /* kcal/mol window above the best mode           */
+    double   hunt_cap[3];     /* (10,10,10), main.cpp:395                      */
+    double   temperature;     /* 1.2                                           */
+    double   amplitude;       /* mutation amplitude 2 (monte_carlo.h:71)       */
+    double   min_rmsd;        /* cluster radius 1.0                            */
+    int32_t  refine;          /* 1 = refine + rescore on the GPU (main.cpp:434)*/
+    int32_t  pad;
+} vd_search_params;
+
+typedef struct {
+    int32_t n_modes;
+    int32_t ntors;
+    float   energy[VD_MAX_MODES];          /* final score, ascending             */
+    float   rmsd_lb[VD_MAX_MODES];         /* to mode 1 (model.cpp:1485-1507)    */
+    float   rmsd_ub[VD_MAX_MODES];
+    float   pose[VD_MAX_MODES][7 + VD_MAX_TORS];
+    int64_t bfgs_evals;                    /* energy+gradient evaluations        */
+} vd_dock_result;
+
+typedef struct {
+    int64_t bfgs_evals;          /* since the context was created               */
+    double  grid_ms;             /* last vd_build_grids kernel time             */
+    double  dock_ms;             /* last docking kernel time                    */
+    double  post_ms;             /* last cluster+refine+rescore kernels time    */
+    int32_t dock_warps_per_block;/* launch shape picked by the autotuner        */
+    int32_t dock_blocks;
+} vd_stats;
+
+/* ---- context ------------------------------------------------------------ */
+vd_status vd_create(vd_ctx** out, int device);
+vd_status vd_destroy(vd_ctx* ctx);
+const char* vd_last_error(void);
+vd_status vd_get_stats(vd_ctx* ctx, vd_stats* out);
+
+/* ---- scoring, receptor, box (main.cpp:337-345, 856-876) ------------------ */
+/* weights: gauss1, gauss2, repulsion, hydrophobic, hydrogen, and the internal
+ * rotor weight 5*w_rot/0.1-1 (main.cpp:862). */
+vd_status vd_set_scoring(vd_ctx* ctx, const double weights[6]);
+vd_status vd_set_receptor(vd_ctx* ctx, int32_t n_atoms, const double* xyz, const int32_t* xs);
+vd_status vd_set_box(vd_ctx* ctx, const double center[3], const double size[3]);
+vd_status vd_grid_dims(vd_ctx* ctx, int32_t npts[3], double begin[3], double end[3]);
+
+/* ---- grid maps: replaces kernel_grid (kernel1.cu:202-249) ----------------- */
+/* Builds one FP32 map per listed XS type over the box; maps stay on device. */
+vd_status vd_build_grids(vd_ctx* ctx, const int32_t* xs_types, int32_t n_types);
+/* Copies one map to the host, x fastest: out[x + nx*(y + ny*z)]. */
+vd_status vd_get_grid(vd_ctx* ctx, int32_t xs_type, float* out);
+
+/* ---- ligands -------------------------------------------------------------- */
+vd_status vd_add_ligand(vd_ctx* ctx, const vd_ligand_desc* lig, int32_t* lig_id);
+vd_status vd_ligand_info(vd_ctx* ctx, int32_t lig_id, int32_t* n_heavy, int32_t* ntors,
+                         int32_t* n_pairs);
+vd_status vd_clear_ligands(vd_ctx* ctx);
+
+/* ---- pose batches: forward energy and adjoint (model.cpp:1324-1333) ------- */
+vd_status vd_energy(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
+                    const vd_eval_params* p, float* e_out);
+vd_status vd_energy_grad(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
+                         const vd_eval_params* p, float* e_out, float* g_out);
+/* Same on device buffers already resident (stream = cudaStream_t or NULL for
+ * the context stream); asynchronous. */
+vd_status vd_energy_grad_device(vd_ctx* ctx, int32_t lig_id, int32_t n_poses,
+                                const float* poses_device, const vd_eval_params* p,
+                                float* e_device, float* g_device, void* stream);
+/* Heavy-atom coordinates of poses (forward kinematics only): [n][n_heavy][3]. */
+vd_status vd_pose_coords(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
+                         float* xyz_out);
+
+/* ---- local optimisation (quasi_newton.cuh:2172-2389, 1710-1806) ------------ */
+/* One RILC-BFGS run per pose on the cached grid; poses are updated in place. */
+vd_status vd_local_opt(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, float* poses,
+                       const vd_eval_params* p, int32_t max_steps, float* e_out,
+                       int64_t* evals);
+
+/* ---- Monte-Carlo search: replaces kernel_monte (kernel2.cu:566-628) -------- */
+/* Raw per-chain best poses and energies of one ligand (one launch).  poses:
+ * [n_chains][7+ntors], e: [n_chains].  Chains use Philox streams keyed by
+ * (seed, lig_id, chain), so the batched and plain forms give equal chains. */
+vd_status vd_mc_chains(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,
+                       float* poses_out, float* e_out, int64_t* evals);
+/* Plain drop-in form: one ligand per launch, then clustering, GPU refinement
+ * and rescoring (main.cpp:423-489). */
+vd_status vd_dock_plain(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,
+                        vd_dock_result* out);
+/* Batched form: all chains of all listed ligands in one persistent launch that
+ * pulls (ligand, chain) items from a device queue; post-processing batched. */
+vd_status vd_dock_batched(vd_ctx* ctx, const int32_t* lig_ids, int32_t n_ligs,
+                          const vd_search_params* sp, vd_dock_result* out);
+
+/* ---- refinement / rescoring on the direct-sum score (non_cache.cpp) -------- */
+/* refine_structure (main.cpp:139-157): dense BFGS with the slope ramp. */
+vd_status vd_refine(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, float* poses,
+                    int32_t max_steps, float* e_out);
+/* eval_adjusted (model.cpp:1428-1431) with intra energy of pose 0 as the
+ * reference, plus the intramolecular energies themselves. */
+vd_status vd_score(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
+                   float* adjusted_out, float* intra_out);
+
+/* ---- host helpers (no GPU work) --------------------------------------------- */
+/* Pair tables built by vd_set_scoring: fast[153][2051], smooth e / dor. */
+vd_status vd_get_tables(vd_ctx* ctx, double* fast, double* smooth_e, double* smooth_dor);
+/* PDBQT ingestion (lib/parse_pdbqt.cpp, lib/model.cpp typing).  Returned
+ * arrays are owned by the handle and live until vd_pdbqt_free. */
+typedef struct vd_pdbqt vd_pdbqt;
+vd_status vd_pdbqt_ligand(const char* text, vd_pdbqt** out, vd_ligand_desc* desc);
+vd_status vd_pdbqt_receptor(const char* text, vd_pdbqt** out, int32_t* n_atoms,
+                            const double** xyz, const int32_t** xs);
+/* Writes a docked model: the input ligand text with coordinates replaced
+ * (model.cpp:1088-1116); xyz_all holds every ligand atom [n_atoms][3]. */
+vd_status vd_pdbqt_write_model(vd_pdbqt* lig, const double* xyz_all, char* buf, int64_t buf_size,
+                               int64_t* written);
+vd_status vd_pdbqt_free(vd_pdbqt* h);
+/* All-atom coordinates (hydrogens included) for a pose, on the host, from the
+ * descriptor (tree.h:395-400 set_conf), for writing output files. */
+vd_status vd_conf_to_coords(const vd_ligand_desc* lig, const float* pose, double* xyz_all);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VDOCK_H */

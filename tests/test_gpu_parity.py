@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances (written here, used below):
+* grid maps:  |gpu - oracle| <= 1e-5 * max(|oracle|, 1)     (FP32 maps)
+* energies:   |gpu - oracle| <= 1e-3 kcal/mol for poses whose atoms are
+              inside the grid box; penalty-dominated poses (atoms outside the
+              box, slope 1e6 kcal/mol/A) within 1e-4 relative: FP32 atom
+              coordinates carry ~1e-6 A rounding, i.e. ~1 kcal/mol of penalty
+              on a 1e5 kcal/mol energy
+* gradients:  |gpu - oracle|_inf <= 1e-3 * max(1, |oracle|_inf)
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+GRID_TOL = 1e-5
+E_TOL = 1e-3
+G_TOL = 1e-3
+
+
+@pytest.fixture(scope="module")
+def vd():
+    if not has_gpu():
+        pytest.skip("needs a CUDA device")
+    import vdock
+    return vdock
+
+
+def setup_pair(vd, rec_atoms=600, radius=20.0, box=12.0, seed=1):
+    from vdock import synth
+    xyz, xs = synth.receptor(rec_atoms, radius, seed)
+    ctx = vd.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0.0, 0.0, 0.0], [box] * 3)
+    orc = O.Oracle()
+    orc.set_receptor(xyz, xs)
+    orc.set_box([0.0, 0.0, 0.0], [box] * 3)
+    return ctx, orc, xyz, xs
+
+
+def test_grid_maps_match_oracle(vd):
+    from vdock import synth
+    ctx, orc, _, _ = setup_pair(vd, rec_atoms=1500, radius=25.0, box=10.0)
+    types = synth.TYPES8
+    ctx.build_grids(types)
+    orc.build_grids(types)
+    for t in types:
+        g = ctx.grid(t).astype(np.float64)
+        r = orc.grid(t)
+        err = np.abs(g - r) / np.maximum(np.abs(r), 1.0)
+        assert err.max() <= GRID_TOL, (t, err.max())
+
+
+def test_grid_all_17_types_and_odd_box(vd):
+    ctx, orc, _, _ = setup_pair(vd, rec_atoms=800, radius=20.0, box=7.1)
+    ctx.set_box([0.3, -0.2, 0.1], [7.1, 5.3, 6.2])
+    orc.set_box([0.3, -0.2, 0.1], [7.1, 5.3, 6.2])
+    types = list(range(17))
+    ctx.build_grids(types)
+    orc.build_grids(types)
+    for t in types:
+        g = ctx.grid(t).astype(np.float64)
+        r = orc.grid(t)
+        assert g.shape == r.shape
+        err = np.abs(g - r) / np.maximum(np.abs(r), 1.0)
+        assert err.max() <= GRID_TOL, (t, err.max())
+
+
+def make_ligand_ctx(vd, n_atoms=40, n_tors=10, box=24.0, seed=3):
+    from vdock import synth
+    ctx, orc, _, _ = setup_pair(vd, rec_atoms=2000, radius=30.0, box=box)
+    lig = synth.ligand(n_atoms, n_tors, seed)
+    types = sorted(set(int(t) for t in lig["xs"]))
+    ctx.build_grids(types)
+    orc.build_grids(types)
+    lc = ctx.add_ligand(lig)
+    lo = orc.add_ligand(lig)
+    return ctx, orc, lig, lc, lo
+
+
+def in_box(orc, lo, poses, n_atoms):
+    _, b, e = orc.grid_info()
+    ok = []
+    for p in poses:
+        x = orc.coords(lo, p.astype(np.float64), n_atoms)
+        ok.append(bool(np.all(x >= b) and np.all(x <= e)))
+    return np.array(ok)
+
+
+def test_energy_and_gradient_match_oracle(vd):
+    from vdock import synth
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd)
+    nt = ctx.ntors[lc]
+    poses = synth.random_poses(256, nt, -4.0, 4.0, seed=7)
+    for v, slope in (((10, 10, 10), 1e6), ((1000, 1000, 1000), 1e6)):
+        ep = vd.eval_params(v[0], v[1], slope)
+        e_gpu, g_gpu = ctx.energy_grad(lc, poses, ep)
+        e_only = ctx.energy(lc, poses, ep)
+        np.testing.assert_allclose(e_only, e_gpu, rtol=0, atol=1e-5 * np.abs(e_gpu).max())
+        inside = in_box(orc, lo, poses, lig["n_atoms"])
+        assert inside.sum() >= 64
+        for i, p in enumerate(poses):
+            e_ref, g_ref = orc.eval_deriv(lo, p.astype(np.float64), v=v, slope=slope)
+            if inside[i]:
+                assert abs(e_gpu[i] - e_ref) <= E_TOL, (i, e_gpu[i], e_ref)
+            else:
+                assert abs(e_gpu[i] - e_ref) <= 1e-4 * abs(e_ref) + E_TOL, (i, e_gpu[i], e_ref)
+            assert np.abs(g_gpu[i] - g_ref).max() <= G_TOL * max(1.0, np.abs(g_ref).max()), (i, g_gpu[i], g_ref)
+
+
+def test_energy_is_deterministic(vd):
+    from vdock import synth
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, seed=5)
+    poses = synth.random_poses(512, ctx.ntors[lc], -4.0, 4.0, seed=9)
+    a = ctx.energy_grad(lc, poses)
+    b = ctx.energy_grad(lc, poses)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_pose_coords_match_oracle(vd):
+    from vdock import synth
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, seed=11)
+    poses = synth.random_poses(64, ctx.ntors[lc], -4.0, 4.0, seed=2)
+    x = ctx.pose_coords(lc, poses)
+    heavy = lig["xs"] >= 0
+    for i, p in enumerate(poses):
+        ref = orc.coords(lo, p.astype(np.float64), lig["n_atoms"])[heavy]
+        np.testing.assert_allclose(x[i], ref, atol=2e-4)
+
+
+def test_local_opt_matches_oracle_rilc(vd):
+    """RILC-BFGS from identical in-box starts.  Each returned energy is the
+    energy of the returned pose; FP32 and FP64 runs then agree as
+    distributions (paired median difference <= 0.1 kcal/mol, two-sample KS
+    p >= 0.01); single runs may end in different minima because rounding
+    changes the line-search path."""
+    from scipy.stats import ks_2samp
+    from vdock import synth
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, seed=13, box=30.0)
+    poses = synth.random_poses(128, ctx.ntors[lc], -1.0, 1.0, seed=4)
+    e_gpu, p_gpu, ev = ctx.local_opt(lc, poses, 20)
+    assert ev > 0
+    e_ref = np.array([orc.rilc_bfgs(lo, p.astype(np.float64), 20)[0] for p in poses])
+    for i in range(0, len(poses), 8):
+        g_e, _ = orc.eval_deriv(lo, p_gpu[i].astype(np.float64))
+        assert abs(g_e - e_gpu[i]) <= 1e-3 + 1e-6 * abs(g_e)
+    assert abs(np.median(e_gpu - e_ref)) <= 0.1, np.median(e_gpu - e_ref)
+    assert ks_2samp(e_gpu, e_ref).pvalue >= 0.01
+
+
+def test_mc_initial_poses_share_streams_with_oracle(vd):
+    """A negative search_depth returns each chain's initial pose: the Philox draws
+    (position in the box, normalised 4-D Gaussian rotation, torsions) are
+    the oracle's to FP32 rounding."""
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=20, n_tors=4, seed=17)
+    sp = vd.search_params(seed=42, n_chains=64, search_depth=-1)
+    p_gpu, e_gpu, _ = ctx.mc_chains(lc, sp)
+    for ch in range(64):
+        ref = orc.init_conf(lo, 42, lc, ch)
+        np.testing.assert_allclose(p_gpu[ch], ref, atol=2e-5)
+
+
+def test_mc_chains_match_oracle_distribution(vd):
+    """Best-of-chain energies of the GPU search and of the oracle's double
+    restatement of the same search (kernel2.cu:219-426) with the same seeds:
+    each returned energy is its pose's energy, paired median difference
+    <= 0.15 kcal/mol and two-sample KS p >= 0.01."""
+    from scipy.stats import ks_2samp
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=20, n_tors=4, seed=17, box=16.0)
+    sp = vd.search_params(seed=42, n_chains=192, search_depth=4, max_bfgs_steps=15)
+    p_gpu, e_gpu, ev = ctx.mc_chains(lc, sp)
+    assert ev > 0 and np.all(np.isfinite(e_gpu))
+    conf, e_ref, _ = orc.mc_chains(lo, 42, lc, 4, 15, 0, 192, threads=8)
+    for i in range(0, 192, 16):
+        g_e, _ = orc.eval_deriv(lo, p_gpu[i].astype(np.float64))
+        assert abs(g_e - e_gpu[i]) <= 1e-3 + 1e-6 * abs(g_e)
+    assert abs(np.median(e_gpu - e_ref)) <= 0.15, np.median(e_gpu - e_ref)
+    assert ks_2samp(e_gpu, e_ref).pvalue >= 0.01
+
+
+def test_plain_and_batched_forms_compute_identical_chains(vd):
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=18, n_tors=3, seed=19)
+    sp = vd.search_params(seed=3, n_chains=64, search_depth=3, max_bfgs_steps=10, refine=0)
+    r_plain = ctx.dock_plain(lc, sp)
+    r_batch = ctx.dock_batched([lc], sp)[0]
+    np.testing.assert_array_equal(r_plain["energy"], r_batch["energy"])
+    np.testing.assert_array_equal(r_plain["pose"], r_batch["pose"])

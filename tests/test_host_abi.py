@@ -1,0 +1,179 @@
+"""Host-side checks that need no GPU: the C-ABI library loads and exports
+every entry point include/vdock.h declares, and its PDBQT ingestion,
+typing, pair selection and host kinematics agree with the oracle."""
+import ctypes as C
+import gzip
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+import pdbqt_oracle as P
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import vdock
+    return vdock.lib()
+
+
+def header_functions():
+    text = open(os.path.join(REPO, "include", "vdock.h")).read()
+    return sorted(set(re.findall(r"\b(vd_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_entry_point(lib):
+    names = header_functions()
+    assert len(names) >= 25
+    for n in names:
+        assert hasattr(lib, n), n
+    import vdock
+    assert set(vdock.EXPORTS) <= set(names)
+
+
+def fixture_text(golden_dir, name):
+    return gzip.open(os.path.join(golden_dir, "pdbqt", name + ".gz"), "rt").read()
+
+
+def parse_with_lib(lib, text):
+    import vdock
+    h = C.c_void_p()
+    d = vdock.LigandDesc()
+    lib.vd_pdbqt_ligand.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(vdock.LigandDesc)]
+    lib.vd_pdbqt_ligand.restype = C.c_int
+    st = lib.vd_pdbqt_ligand(text.encode(), C.byref(h), C.byref(d))
+    assert st == 0, lib.vd_last_error()
+    na, nn, npair = d.n_atoms, d.n_nodes, d.n_pairs
+    arr = lambda p, n: np.ctypeslib.as_array(p, shape=(n,)).copy()
+    out = dict(n_atoms=na, xyz=arr(d.xyz, 3 * na).reshape(-1, 3), xs=arr(d.xs, na), el=arr(d.el, na),
+               atom_node=arr(d.atom_node, na), node_parent=arr(d.node_parent, nn),
+               node_origin_atom=arr(d.node_origin_atom, nn), node_axis_atom=arr(d.node_axis_atom, nn),
+               pairs=arr(d.pairs, 2 * npair).reshape(-1, 2), num_tors=d.num_tors)
+    return h, d, out
+
+
+@pytest.mark.parametrize("name", ["1u1b_ligand.pdbqt", "2bm2_ligand.pdbqt", "2er7_ligand.pdbqt"])
+def test_ligand_parse_matches_oracle(lib, golden_dir, name):
+    text = fixture_text(golden_dir, name)
+    h, d, got = parse_with_lib(lib, text)
+    ref = P.parse_ligand(text).descriptor()
+    for k in ("xs", "el", "atom_node", "node_parent", "node_origin_atom", "node_axis_atom", "pairs"):
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    np.testing.assert_array_equal(got["xyz"], ref["xyz"])
+    assert got["num_tors"] == ref["num_tors"]
+    lib.vd_pdbqt_free(h)
+
+
+def test_receptor_parse_matches_oracle(lib, golden_dir):
+    text = fixture_text(golden_dir, "1u1b_protein.pdbqt")
+    h = C.c_void_p()
+    n = C.c_int32()
+    xyz = C.POINTER(C.c_double)()
+    xs = C.POINTER(C.c_int32)()
+    lib.vd_pdbqt_receptor.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int32),
+                                      C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_int32))]
+    assert lib.vd_pdbqt_receptor(text.encode(), C.byref(h), C.byref(n), C.byref(xyz), C.byref(xs)) == 0
+    z = np.load(os.path.join(golden_dir, "kat_vina.npz"))
+    np.testing.assert_array_equal(np.ctypeslib.as_array(xs, shape=(n.value,)), z["rec_xs"])
+    np.testing.assert_array_equal(np.ctypeslib.as_array(xyz, shape=(3 * n.value,)).reshape(-1, 3), z["rec_xyz"])
+    lib.vd_pdbqt_free(h)
+
+
+def test_parse_errors_are_reported(lib):
+    import vdock
+    h = C.c_void_p()
+    d = vdock.LigandDesc()
+    bad = "ROOT\nATOM      1  C   UNL     1       0.000   0.000   0.000  0.00  0.00    +0.000 Xx\nENDROOT\nTORSDOF 0\n"
+    assert lib.vd_pdbqt_ligand(bad.encode(), C.byref(h), C.byref(d)) == 5  # VD_ERR_PARSE
+    assert b"not a valid AutoDock type" in lib.vd_last_error()
+    missing = "ROOT\nATOM      1  C   UNL     1       0.000   0.000   0.000  0.00  0.00    +0.000 C \nENDROOT\n"
+    assert lib.vd_pdbqt_ligand(missing.encode(), C.byref(h), C.byref(d)) == 5
+    assert b"TORSDOF" in lib.vd_last_error()
+
+
+def test_conf_to_coords_matches_oracle_and_writer_round_trips(lib, golden_dir):
+    import vdock
+    text = fixture_text(golden_dir, "1u1b_ligand.pdbqt")
+    h, d, got = parse_with_lib(lib, text)
+    orc = O.Oracle()
+    orc.set_receptor(np.zeros((1, 3)), np.array([0], np.int32))
+    orc.set_box([0, 0, 0], [10, 10, 10])
+    lid = orc.add_ligand(got)
+    nt = orc.ntors[lid]
+    rng = np.random.default_rng(0)
+    lib.vd_conf_to_coords.argtypes = [C.POINTER(vdock.LigandDesc), C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    for _ in range(5):
+        pose = np.concatenate([rng.uniform(-5, 5, 3), rng.normal(size=4), rng.uniform(-3, 3, nt)]).astype(np.float32)
+        pose[3:7] /= np.linalg.norm(pose[3:7])
+        out = np.zeros(3 * got["n_atoms"])
+        assert lib.vd_conf_to_coords(C.byref(d), pose.ctypes.data_as(C.POINTER(C.c_float)),
+                                     out.ctypes.data_as(C.POINTER(C.c_double))) == 0
+        ref = orc.coords(lid, pose.astype(np.float64), got["n_atoms"])
+        # the oracle uses the FP32 quaternion unnormalised (|q|^2 - 1 ~ 1e-7)
+        np.testing.assert_allclose(out.reshape(-1, 3), ref, atol=1e-5)
+    # writing the input coordinates reproduces the input atom lines
+    n = C.c_int64()
+    lib.vd_pdbqt_write_model.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_char_p, C.c_int64, C.POINTER(C.c_int64)]
+    xyz = np.ascontiguousarray(got["xyz"].ravel())
+    assert lib.vd_pdbqt_write_model(h, xyz.ctypes.data_as(C.POINTER(C.c_double)), None, 0, C.byref(n)) == 0
+    buf = C.create_string_buffer(n.value + 1)
+    assert lib.vd_pdbqt_write_model(h, xyz.ctypes.data_as(C.POINTER(C.c_double)), buf, n.value + 1, C.byref(n)) == 0
+    assert buf.value.decode().splitlines() == [s.rstrip("\r") for s in text.splitlines()]
+    lib.vd_pdbqt_free(h)
+
+
+def test_synthetic_ligand_topology_follows_reference_rules():
+    """Written as PDBQT and re-parsed by the oracle's restatement of the
+    reference parser (bonds perceived from distances), a synthetic ligand
+    yields the same rigid bodies, intra pairs and N_tors as the generator."""
+    from vdock import synth
+    for seed in range(6):
+        lig = synth.ligand(30, 6, seed)
+        ref_lig = P.parse_ligand(to_pdbqt(lig))
+        ref = ref_lig.descriptor()
+        assert len(ref["node_parent"]) == len(lig["node_parent"])
+        num = np.array([a.number - 1 for a in ref_lig.atoms])
+        got_pairs = {tuple(sorted((int(num[a]), int(num[b])))) for a, b in ref["pairs"]}
+        want = {tuple(sorted((int(a), int(b)))) for a, b in lig["pairs"]}
+        assert got_pairs == want
+        assert ref["num_tors"] == lig["num_tors"]
+
+
+def to_pdbqt(lig):
+    """ROOT/BRANCH writer for a generated ligand (test helper); a branch
+    block starts with its origin atom, as the reference expects."""
+    el_name = {1: "C", 2: "N", 3: "O", 4: "S"}
+    ad = {0: "C", 1: "C", 2: "N", 3: "N", 4: "NA", 8: "OA", 9: "OA", 10: "S"}
+    xyz, node, parent = lig["xyz"], lig["atom_node"], lig["node_parent"]
+    origin, axis = lig["node_origin_atom"], lig["node_axis_atom"]
+    child_origins = set(int(origin[c]) for c in range(1, len(parent)))
+    lines = []
+
+    def atom(i):
+        x, y, z = xyz[i]
+        t = ad[int(lig["xs"][i])]
+        return (f"ATOM  {i + 1:5d}  {el_name[int(lig['el'][i])]:<3s} LIG     1    "
+                f"{x:8.3f}{y:8.3f}{z:8.3f}  0.00  0.00    +0.000 {t:<2s}")
+
+    def body_atoms(k):
+        return [i for i in np.where(node == k)[0] if int(i) not in child_origins]
+
+    def branches(k):
+        for c in np.where(parent == k)[0]:
+            lines.append(f"BRANCH {axis[c] + 1:3d} {origin[c] + 1:3d}")
+            lines.append(atom(origin[c]))
+            for i in body_atoms(c):
+                lines.append(atom(i))
+            branches(c)
+            lines.append(f"ENDBRANCH {axis[c] + 1:3d} {origin[c] + 1:3d}")
+    lines.append("ROOT")
+    for i in body_atoms(0):
+        lines.append(atom(i))
+    lines.append("ENDROOT")
+    branches(0)
+    lines.append(f"TORSDOF {len(parent) - 1}")
+    return "\n".join(lines) + "\n"

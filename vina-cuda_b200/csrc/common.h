@@ -1,0 +1,157 @@
+// Internal declarations shared by the vdock host code and CUDA kernels.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/vdock.h"
+
+namespace vd {
+
+constexpr int kTypes = 17;                       // XS_TYPE_SIZE
+constexpr int kPairTypes = kTypes * (kTypes + 1) / 2;  // 153
+constexpr int kN = 2051;                         // int(32*64)+3 table entries
+constexpr int kBins = 2049;                      // bins reachable for r^2 <= 64
+constexpr double kCutoff2 = 64.0;
+constexpr int kMaxHeavy = VD_MAX_ATOMS;
+constexpr int kMaxTors = VD_MAX_TORS;
+constexpr int kMaxNodes = VD_MAX_TORS + 1;
+constexpr int kMaxPairs = VD_MAX_PAIRS;
+
+inline int tri_index(int t1, int t2) {
+    return (t1 <= t2) ? t1 + t2 * (t2 + 1) / 2 : t2 + t1 * (t1 + 1) / 2;
+}
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& msg);
+#define VD_CUDA(call)                                                              \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            ::vd::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));   \
+            return VD_ERR_CUDA;                                                    \
+        }                                                                          \
+    } while (0)
+#define VD_CHECK(cond, code, msg)                                                  \
+    do {                                                                           \
+        if (!(cond)) {                                                             \
+            ::vd::set_error(msg);                                                  \
+            return code;                                                           \
+        }                                                                          \
+    } while (0)
+
+// ---------------------------------------------------------------- device ligand
+// One ligand is one contiguous blob of 16-byte words in the ligand pool:
+//   LigHeader | atoms (float4) | nodes (NodeRec) | pairs (int2) |
+//   csr offsets (int, n_heavy+1, padded) | csr entries (int, padded)
+// Only heavy atoms (XS type >= 0) are on the device; hydrogens carry no
+// energy and are placed on the host when output files are written.
+struct LigHeader {
+    int32_t n_atoms;      // heavy atoms
+    int32_t n_nodes;
+    int32_t n_pairs;
+    int32_t ntors;
+    int32_t off_atoms;    // in 16-byte words from the blob start
+    int32_t off_nodes;
+    int32_t off_pairs;    // int2 entries start (16-byte word offset)
+    int32_t off_csr;      // int entries start (16-byte word offset)
+    int32_t off_csr_list;
+    int32_t max_depth;
+    int32_t n_csr;        // 2*n_pairs
+    int32_t pad0;
+    float conf_indep;     // 1 / (1 + w*num_tors/5)
+    float pad1, pad2, pad3;
+};
+static_assert(sizeof(LigHeader) == 64, "header size");
+
+// Atom word: local coords (relative to its rigid body's origin) and
+// (xs type | node << 8) stored in .w as int bits.
+// Rigid body record: origin relative to parent frame, torsion axis in the
+// parent frame, parent index, atom range and subtree end (pre-order).
+struct NodeRec {
+    float rel_origin[3];
+    float axis[3];
+    int32_t parent;
+    int32_t atom_begin;
+    int32_t atom_end;
+    int32_t subtree_end;  // nodes [k, subtree_end) form k's subtree
+    int32_t depth;
+    int32_t pad;
+};
+static_assert(sizeof(NodeRec) == 48, "node size");
+
+struct HostLigand {
+    LigHeader h;
+    std::vector<float4> blob;      // whole blob incl. header
+    // host-side copies for helpers
+    std::vector<int32_t> heavy_index;  // device atom -> input atom index
+    int32_t n_all_atoms = 0;
+    int64_t pool_offset = 0;       // in float4 words
+    double num_tors = 0;
+};
+
+// Grid geometry exactly as main.cpp:864-876 / grid.cpp:29-43 (double).
+struct GridGeom {
+    int32_t n[3];          // points per dim
+    double begin[3], end[3];
+    double init[3], factor[3], finv[3], dmo[3];
+    int32_t pitch;         // x pitch in floats (multiple of 4)
+};
+
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool scoring = false;
+    double weights[6];
+    std::vector<double> fast, se, sd;     // [153][2051] double (host)
+    float* d_fast = nullptr;              // [153][2049] float (rescoring, eval_fast)
+    float4* d_smooth = nullptr;           // [153][2049] {e_i, dor_i, e_i+1, dor_i+1}
+    double* d_fastd = nullptr;            // [153][2049] double (final rescoring)
+    // receptor
+    std::vector<double> rec_xyz;
+    std::vector<int32_t> rec_xs;
+    bool has_box = false;
+    GridGeom geom{};
+    // grids
+    float* d_maps = nullptr;              // [n_maps][nz][ny][pitch]
+    size_t map_stride = 0;                // floats per map
+    int map_slot[kTypes];                 // xs type -> map index or -1
+    int n_maps = 0;
+    // direct-sum receptor cell list (non_cache): ~3 A cells over the box,
+    // each listing the receptor atoms within 8 A of it (szv_grid.cpp:28-74)
+    float4* d_rec = nullptr;              // relevant receptor atoms {x,y,z,type}
+    double4* d_recd = nullptr;            // same in double
+    int32_t* d_cell_start = nullptr;      // [cells+1]
+    int32_t* d_cell_list = nullptr;       // atom indices
+    int32_t cell_dim[3] = {0, 0, 0};
+    double cell_init[3], cell_range[3];
+    int32_t n_rec_dev = 0;
+    bool rec_dev_ready = false;
+    // ligands
+    std::vector<HostLigand> ligs;
+    float4* d_pool = nullptr;
+    int64_t pool_words = 0, pool_cap = 0;
+    bool pool_dirty = false;
+    // scratch
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int32_t* d_counter = nullptr;         // work queue + error words
+    vd_stats stats{};
+};
+
+vd_status ensure_scratch(Ctx* c, size_t bytes);
+vd_status sync_pool(Ctx* c);
+vd_status ensure_receptor_cells(Ctx* c);
+void build_tables(const double w[6], std::vector<double>& fast, std::vector<double>& se,
+                  std::vector<double>& sd);
+
+}  // namespace vd
+
+struct vd_ctx {
+    vd::Ctx c;
+};

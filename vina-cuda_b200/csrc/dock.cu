@@ -1,0 +1,265 @@
+// Monte-Carlo search: replaces kernel_monte / kernel2_update (kernel2.cu:219-426).
+//
+// One warp runs one chain: `search_depth` steps of mutate -> RILC-BFGS ->
+// Metropolis (T = 1.2), re-optimising an accepted pose that beats the
+// chain's best, exactly the control flow of kernel2.cu:290-421.  Random
+// numbers come from a Philox stream keyed by (seed, ligand, chain), so the
+// plain (one ligand per launch, one warp per chain) and the batched
+// (persistent, work queue over (ligand, chain) items) forms compute the same
+// chains.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "dock.h"
+#include "launch.h"
+#include "search.cuh"
+
+namespace vd {
+namespace {
+
+struct DockParams {
+    const float4* pool;
+    const int64_t* lig_off;      // [n_ligs] blob offsets, in batch order
+    const int32_t* prefix;       // [n_ligs+1] first item of each ligand
+    const uint32_t* lig_uid;     // [n_ligs] Philox stream id
+    const int32_t* depth;        // [n_ligs]
+    const int32_t* bfgs_steps;   // [n_ligs]
+    int32_t n_ligs;
+    int32_t total_items;
+    MapView G;
+    const float4* smooth;
+    EvalParams ep;
+    uint32_t seed;
+    float temperature, amplitude;
+    float lo[3], hi[3];
+    float* out_conf;             // [items][stride]
+    int32_t stride;
+    float* out_e;                // [items]
+    int32_t* queue;
+    unsigned long long* evals;
+    int32_t warp_floats;
+    int32_t warps_per_block;
+};
+
+__device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int item) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {  // last ligand with prefix <= item
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&prefix[mid]) <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <bool persistent>
+__global__ void __launch_bounds__(256) dock_kernel(DockParams p) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float* base = reinterpret_cast<float*>(smem4) + size_t(wid) * p.warp_floats;
+    int evals = 0;
+    int item = persistent ? 0 : blockIdx.x * p.warps_per_block + wid;
+    for (;;) {
+        if (persistent) {
+            int v = 0;
+            if (lane == 0) v = atomicAdd(p.queue, 1);
+            item = __shfl_sync(0xffffffffu, v, 0);
+        }
+        if (item >= p.total_items) break;
+        const int li = find_ligand(p.prefix, p.n_ligs, item);
+        const uint32_t chain = uint32_t(item - __ldg(&p.prefix[li]));
+        const LigView L = lig_view(p.pool, __ldg(&p.lig_off[li]));
+        const int nc = 7 + L.nt, nc4 = pad4(nc);
+        SearchMem s;
+        s.m = carve(base, L.na, L.nn, L.np, L.nt);
+        s.xp = base + warp_floats(L.na, L.nn, L.np, L.nt);
+        s.xo = s.xp + nc4;
+        float* xt = s.xo + nc4;      // current (accepted) pose
+        float* xb = xt + nc4;        // chain best
+        const uint32_t uid = __ldg(&p.lig_uid[li]);
+        const int depth = __ldg(&p.depth[li]), steps = __ldg(&p.bfgs_steps[li]);
+        init_pose(xt, L.nt, p.seed, uid, chain, p.lo, p.hi, lane);
+        copy_conf(xt, xb, nc, lane);
+        float tmp_e = FLT_MAX, best_e = INFINITY;
+        for (int step = 0; step < depth; ++step) {
+            copy_conf(xt, s.m.x, nc, lane);
+            mutate_pose(L, s.m, p.seed, uid, chain, uint32_t(step), p.amplitude, lane);
+            const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
+            uint32_t b[4];
+            draw(p.seed, uid, chain, uint32_t(step), 1, b);
+            const bool accept =
+                step == 0 || ce < tmp_e || u01(b[1]) < expf((tmp_e - ce) / p.temperature);  // kernel2.cu:63-71
+            if (accept) {
+                tmp_e = ce;
+                if (tmp_e < best_e) {
+                    tmp_e = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
+                    if (tmp_e < best_e) {
+                        best_e = tmp_e;
+                        copy_conf(s.m.x, xb, nc, lane);
+                    }
+                }
+                copy_conf(s.m.x, xt, nc, lane);
+            }
+        }
+        float* dst = p.out_conf + size_t(item) * p.stride;
+        for (int i = lane; i < nc; i += 32) dst[i] = xb[i];
+        if (lane == 0) p.out_e[item] = best_e;
+        __syncwarp();
+        if (!persistent) break;
+    }
+    if (lane == 0 && evals) atomicAdd(p.evals, (unsigned long long)evals);
+}
+
+}  // namespace
+
+// Heuristics of main.cpp:354-391 for RILC-BFGS (atoms = all ligand atoms).
+void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps) {
+    depth = sp.search_depth;
+    if (depth < 0) {  // no MC steps: each chain returns its initial pose
+        depth = 0;
+    } else if (depth == 0) {
+        double t = (0.24 * L.n_all_atoms + 0.29 * L.h.ntors - 3.41) * 2;
+        if (t < 1) t = 1;
+        depth = int(t);
+    }
+    bfgs_steps = sp.max_bfgs_steps > 0 ? sp.max_bfgs_steps : int(unsigned(30 + L.n_all_atoms) / 3);
+}
+
+vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
+                      DockBuffers& out, cudaStream_t stream, int warps_per_block_override) {
+    VD_CHECK(!ligs.empty(), VD_ERR_ARG, "no ligands");
+    VD_CHECK(sp.n_chains > 0, VD_ERR_ARG, "n_chains must be positive");
+    VD_CHECK(c.has_box, VD_ERR_ARG, "no box set");
+    vd_status st = sync_pool(&c);
+    if (st != VD_OK) return st;
+    DockParams p{};
+    st = make_map_view(c, p.G);
+    if (st != VD_OK) return st;
+    const int n = int(ligs.size());
+    std::vector<int64_t> off(n);
+    std::vector<int32_t> prefix(n + 1, 0), depth(n), steps(n);
+    std::vector<uint32_t> uid(n);
+    int max_wf = 0, max_nt = 0;
+    for (int i = 0; i < n; ++i) {
+        st = check_ligand_maps(c, ligs[i]);
+        if (st != VD_OK) return st;
+        const HostLigand& L = c.ligs[ligs[i]];
+        off[i] = L.pool_offset;
+        uid[i] = uint32_t(ligs[i]);
+        search_defaults(L, sp, depth[i], steps[i]);
+        prefix[i + 1] = prefix[i] + sp.n_chains;
+        max_wf = std::max(max_wf, lig_warp_floats(L) + 4 * pad4(7 + L.h.ntors));
+        max_nt = std::max(max_nt, L.h.ntors);
+    }
+    const int items = prefix[n];
+    out.items = items;
+    out.stride = 7 + max_nt;
+    out.prefix = prefix;
+    // device buffers: params arrays + outputs
+    const size_t b_off = n * sizeof(int64_t), b_pre = (n + 1) * sizeof(int32_t), b_arr = n * sizeof(int32_t);
+    const size_t b_conf = size_t(items) * out.stride * sizeof(float), b_e = size_t(items) * sizeof(float);
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t total = al(b_off) + al(b_pre) + 3 * al(b_arr) + al(b_conf) + al(b_e) + out.extra_bytes;
+    st = ensure_scratch(&c, total);
+    if (st != VD_OK) return st;
+    char* s = static_cast<char*>(c.d_scratch);
+    int64_t* d_off = reinterpret_cast<int64_t*>(s); s += al(b_off);
+    int32_t* d_pre = reinterpret_cast<int32_t*>(s); s += al(b_pre);
+    uint32_t* d_uid = reinterpret_cast<uint32_t*>(s); s += al(b_arr);
+    int32_t* d_depth = reinterpret_cast<int32_t*>(s); s += al(b_arr);
+    int32_t* d_steps = reinterpret_cast<int32_t*>(s); s += al(b_arr);
+    out.d_conf = reinterpret_cast<float*>(s); s += al(b_conf);
+    out.d_e = reinterpret_cast<float*>(s); s += al(b_e);
+    out.d_extra = s;
+    VD_CUDA(cudaMemcpyAsync(d_off, off.data(), b_off, cudaMemcpyHostToDevice, stream));
+    VD_CUDA(cudaMemcpyAsync(d_pre, prefix.data(), b_pre, cudaMemcpyHostToDevice, stream));
+    VD_CUDA(cudaMemcpyAsync(d_uid, uid.data(), b_arr, cudaMemcpyHostToDevice, stream));
+    VD_CUDA(cudaMemcpyAsync(d_depth, depth.data(), b_arr, cudaMemcpyHostToDevice, stream));
+    VD_CUDA(cudaMemcpyAsync(d_steps, steps.data(), b_arr, cudaMemcpyHostToDevice, stream));
+    VD_CUDA(cudaMemsetAsync(c.d_counter, 0, 16, stream));
+    p.pool = c.d_pool;
+    p.lig_off = d_off;
+    p.prefix = d_pre;
+    p.lig_uid = d_uid;
+    p.depth = d_depth;
+    p.bfgs_steps = d_steps;
+    p.n_ligs = n;
+    p.total_items = items;
+    p.smooth = c.d_smooth;
+    p.ep = {float(sp.hunt_cap[0]), float(sp.hunt_cap[1]), 1e6f};
+    p.seed = sp.seed;
+    p.temperature = float(sp.temperature > 0 ? sp.temperature : 1.2);
+    p.amplitude = float(sp.amplitude > 0 ? sp.amplitude : 2.0);
+    for (int d = 0; d < 3; ++d) {
+        p.lo[d] = float(c.geom.begin[d]);
+        p.hi[d] = float(c.geom.end[d]);
+    }
+    p.out_conf = out.d_conf;
+    p.stride = out.stride;
+    p.out_e = out.d_e;
+    p.queue = c.d_counter;
+    p.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 2);
+    p.warp_floats = max_wf;
+    // launch shape: warps per block from the override / autotuner, as many
+    // resident blocks as fit for the persistent form
+    int wpb = warps_per_block_override > 0 ? warps_per_block_override : 4;
+    while (wpb > 1 && size_t(max_wf) * wpb * 4 > 200 * 1024) wpb >>= 1;
+    const size_t smem = size_t(max_wf) * wpb * sizeof(float);
+    VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "ligand too large for the docking kernel");
+    p.warps_per_block = wpb;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+    VD_CUDA(cudaEventRecord(c.ev0, stream));
+    if (persistent) {
+        auto k = dock_kernel<true>;
+        VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        int per_sm = 0;
+        VD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * wpb, smem));
+        per_sm = std::max(1, per_sm);
+        const int blocks = std::min(sms * per_sm, (items + wpb - 1) / wpb);
+        k<<<blocks, 32 * wpb, smem, stream>>>(p);
+        c.stats.dock_blocks = blocks;
+    } else {
+        auto k = dock_kernel<false>;
+        VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        const int blocks = (items + wpb - 1) / wpb;
+        k<<<blocks, 32 * wpb, smem, stream>>>(p);
+        c.stats.dock_blocks = blocks;
+    }
+    VD_CUDA(cudaGetLastError());
+    VD_CUDA(cudaEventRecord(c.ev1, stream));
+    c.stats.dock_warps_per_block = wpb;
+    return VD_OK;
+}
+
+}  // namespace vd
+
+using namespace vd;
+
+extern "C" {
+
+vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float* poses_out, float* e_out,
+                       int64_t* evals) {
+    VD_CHECK(h && sp && poses_out && e_out, VD_ERR_ARG, "vd_mc_chains: NULL argument");
+    Ctx& c = h->c;
+    VD_CHECK(lig >= 0 && lig < int(c.ligs.size()), VD_ERR_ARG, "vd_mc_chains: bad ligand id");
+    VD_CUDA(cudaSetDevice(c.device));
+    DockBuffers b;
+    vd_status st = launch_dock(c, {lig}, *sp, false, b, c.stream, 0);
+    if (st != VD_OK) return st;
+    const int nc = 7 + c.ligs[lig].h.ntors;
+    VD_CUDA(cudaMemcpy2DAsync(poses_out, nc * sizeof(float), b.d_conf, b.stride * sizeof(float), nc * sizeof(float),
+                              b.items, cudaMemcpyDeviceToHost, c.stream));
+    VD_CUDA(cudaMemcpyAsync(e_out, b.d_e, b.items * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    unsigned long long ev = 0;
+    VD_CUDA(cudaMemcpyAsync(&ev, c.d_counter + 2, 8, cudaMemcpyDeviceToHost, c.stream));
+    VD_CUDA(cudaStreamSynchronize(c.stream));
+    float ms = 0;
+    VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+    c.stats.dock_ms = ms;
+    c.stats.bfgs_evals += int64_t(ev);
+    if (evals) *evals = int64_t(ev);
+    return VD_OK;
+}
+
+}  // extern "C"

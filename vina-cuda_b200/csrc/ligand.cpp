@@ -1,0 +1,220 @@
+// Ligand ingestion: validates a vd_ligand_desc and packs the device blob
+// (heavy atoms only, rigid bodies in pre-order, intra pairs and the per-atom
+// incidence lists the force gather uses).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "common.h"
+
+namespace vd {
+
+vd_status sync_pool(Ctx* c) {
+    if (!c->pool_dirty) return VD_OK;
+    int64_t words = 0;
+    for (auto& L : c->ligs) words += int64_t(L.blob.size());
+    if (words > c->pool_cap) {
+        if (c->d_pool) VD_CUDA(cudaFree(c->d_pool));
+        c->d_pool = nullptr;
+        int64_t cap = std::max<int64_t>(words + words / 2, 4096);
+        VD_CUDA(cudaMalloc(&c->d_pool, size_t(cap) * sizeof(float4)));
+        c->pool_cap = cap;
+    }
+    std::vector<float4> host(size_t(std::max<int64_t>(words, 1)));
+    int64_t off = 0;
+    for (auto& L : c->ligs) {
+        L.pool_offset = off;
+        std::memcpy(&host[size_t(off)], L.blob.data(), L.blob.size() * sizeof(float4));
+        off += int64_t(L.blob.size());
+    }
+    VD_CUDA(cudaMemcpyAsync(c->d_pool, host.data(), size_t(words) * sizeof(float4), cudaMemcpyHostToDevice,
+                            c->stream));
+    VD_CUDA(cudaStreamSynchronize(c->stream));
+    c->pool_words = words;
+    c->pool_dirty = false;
+    return VD_OK;
+}
+
+namespace {
+
+// Checks that rigid bodies are numbered in depth-first pre-order, the order
+// in which torsions are stored in a pose (tree.h:395-400).
+bool preorder_ok(const int32_t* parent, int nn) {
+    if (nn < 1 || parent[0] != -1) return false;
+    std::vector<int> stack{0};
+    for (int k = 1; k < nn; ++k) {
+        const int p = parent[k];
+        while (!stack.empty() && stack.back() != p) stack.pop_back();
+        if (stack.empty()) return false;
+        stack.push_back(k);
+    }
+    return true;
+}
+
+}  // namespace
+}  // namespace vd
+
+using namespace vd;
+
+extern "C" {
+
+vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
+    VD_CHECK(h && d && lig_id, VD_ERR_ARG, "vd_add_ligand: NULL argument");
+    Ctx& c = h->c;
+    const int na = d->n_atoms, nn = d->n_nodes, np = d->n_pairs;
+    VD_CHECK(na >= 1 && nn >= 1 && np >= 0, VD_ERR_ARG, "vd_add_ligand: empty ligand");
+    VD_CHECK(d->xyz && d->xs && d->el && d->atom_node && d->node_parent && d->node_origin_atom &&
+                 d->node_axis_atom && (np == 0 || d->pairs),
+             VD_ERR_ARG, "vd_add_ligand: NULL array");
+    VD_CHECK(nn - 1 <= kMaxTors, VD_ERR_CAPACITY, "vd_add_ligand: more than 48 torsions");
+    VD_CHECK(preorder_ok(d->node_parent, nn), VD_ERR_ARG,
+             "vd_add_ligand: rigid bodies must be numbered in depth-first pre-order");
+    std::vector<int32_t> heavy_of(na, -1), heavy_index;
+    for (int i = 0; i < na; ++i) {
+        VD_CHECK(d->xs[i] >= -1 && d->xs[i] < kTypes, VD_ERR_ARG, "vd_add_ligand: XS type out of range");
+        VD_CHECK(d->atom_node[i] >= 0 && d->atom_node[i] < nn, VD_ERR_ARG, "vd_add_ligand: atom_node out of range");
+        VD_CHECK(i == 0 || d->atom_node[i] >= d->atom_node[i - 1], VD_ERR_ARG,
+                 "vd_add_ligand: atoms must be grouped by rigid body in body order");
+        if (d->xs[i] >= 0) {
+            heavy_of[i] = int32_t(heavy_index.size());
+            heavy_index.push_back(i);
+        }
+    }
+    const int nh = int(heavy_index.size());
+    VD_CHECK(nh >= 1, VD_ERR_ARG, "vd_add_ligand: no typed (heavy) atoms");
+    VD_CHECK(nh <= kMaxHeavy, VD_ERR_CAPACITY, "vd_add_ligand: more than 128 heavy atoms");
+    for (int k = 0; k < nn; ++k) {
+        VD_CHECK(d->node_origin_atom[k] >= 0 && d->node_origin_atom[k] < na, VD_ERR_ARG,
+                 "vd_add_ligand: node_origin_atom out of range");
+        VD_CHECK(k == 0 || (d->node_axis_atom[k] >= 0 && d->node_axis_atom[k] < na), VD_ERR_ARG,
+                 "vd_add_ligand: node_axis_atom out of range");
+    }
+    // pairs between heavy atoms
+    std::vector<int2> pairs;
+    for (int p = 0; p < np; ++p) {
+        const int a = d->pairs[2 * p], b = d->pairs[2 * p + 1];
+        VD_CHECK(a >= 0 && a < na && b >= 0 && b < na && a != b, VD_ERR_ARG, "vd_add_ligand: pair index out of range");
+        if (heavy_of[a] < 0 || heavy_of[b] < 0) continue;
+        pairs.push_back(make_int2(heavy_of[a] | (heavy_of[b] << 16), tri_index(d->xs[a], d->xs[b])));
+    }
+    const int P = int(pairs.size());
+    VD_CHECK(P <= kMaxPairs, VD_ERR_CAPACITY, "vd_add_ligand: more than 4096 intra pairs");
+
+    auto xyz = [&](int i, int k) { return d->xyz[3 * size_t(i) + k]; };
+    // body geometry (tree.h:230-262): origin, unit axis from the parent-side atom
+    std::vector<NodeRec> nodes(nn);
+    std::vector<int> depth(nn, 0), sub_end(nn, 0);
+    for (int k = 0; k < nn; ++k) {
+        NodeRec& r = nodes[k];
+        std::memset(&r, 0, sizeof(r));
+        r.parent = d->node_parent[k];
+        depth[k] = (k == 0) ? 0 : depth[r.parent] + 1;
+        r.depth = depth[k];
+        const int o = d->node_origin_atom[k];
+        if (k > 0) {
+            const int po = d->node_origin_atom[r.parent];
+            const int ax = d->node_axis_atom[k];
+            double diff[3], nrm = 0;
+            for (int j = 0; j < 3; ++j) {
+                r.rel_origin[j] = float(xyz(o, j) - xyz(po, j));
+                diff[j] = xyz(o, j) - xyz(ax, j);
+                nrm += diff[j] * diff[j];
+            }
+            nrm = std::sqrt(nrm);
+            VD_CHECK(nrm > 1e-6, VD_ERR_ARG, "vd_add_ligand: zero-length torsion axis");
+            for (int j = 0; j < 3; ++j) r.axis[j] = float((1 / nrm) * diff[j]);
+        }
+        r.atom_begin = nh;
+        r.atom_end = 0;
+    }
+    for (int k = nn - 1; k >= 0; --k) {  // pre-order: subtree is [k, sub_end)
+        sub_end[k] = k + 1;
+        for (int j = k + 1; j < nn && depth[j] > depth[k]; ++j) sub_end[k] = j + 1;
+    }
+    int max_depth = 0;
+    for (int k = 0; k < nn; ++k) {
+        nodes[k].subtree_end = sub_end[k];
+        max_depth = std::max(max_depth, depth[k]);
+    }
+    std::vector<float4> atoms(nh);
+    for (int hi = 0; hi < nh; ++hi) {
+        const int i = heavy_index[hi];
+        const int k = d->atom_node[i];
+        const int o = d->node_origin_atom[k];
+        NodeRec& r = nodes[k];
+        r.atom_begin = std::min(r.atom_begin, hi);
+        r.atom_end = std::max(r.atom_end, hi + 1);
+        float4 a;
+        a.x = float(xyz(i, 0) - xyz(o, 0));
+        a.y = float(xyz(i, 1) - xyz(o, 1));
+        a.z = float(xyz(i, 2) - xyz(o, 2));
+        VD_CHECK(d->el[i] >= 0 && d->el[i] < 256, VD_ERR_ARG, "vd_add_ligand: element type out of range");
+        int packed = d->xs[i] | (k << 8) | (d->el[i] << 16);
+        std::memcpy(&a.w, &packed, sizeof(int));
+        atoms[hi] = a;
+    }
+    for (auto& r : nodes)
+        if (r.atom_begin > r.atom_end) r.atom_begin = r.atom_end = 0;
+    // incidence lists: entry = pair << 1 | (atom is the pair's second atom)
+    std::vector<std::vector<int>> inc(nh);
+    for (int p = 0; p < P; ++p) {
+        inc[pairs[p].x & 0xffff].push_back(p << 1);
+        inc[pairs[p].x >> 16].push_back((p << 1) | 1);
+    }
+    std::vector<int32_t> csr_off(nh + 1, 0), csr;
+    for (int i = 0; i < nh; ++i) {
+        csr_off[i + 1] = csr_off[i] + int(inc[i].size());
+        csr.insert(csr.end(), inc[i].begin(), inc[i].end());
+    }
+
+    HostLigand L;
+    LigHeader& H = L.h;
+    std::memset(&H, 0, sizeof(H));
+    H.n_atoms = nh;
+    H.n_nodes = nn;
+    H.n_pairs = P;
+    H.ntors = nn - 1;
+    H.max_depth = max_depth;
+    H.n_csr = int(csr.size());
+    auto words = [](size_t bytes) { return int32_t((bytes + 15) / 16); };
+    H.off_atoms = 4;
+    H.off_nodes = H.off_atoms + nh;
+    H.off_pairs = H.off_nodes + 3 * nn;
+    H.off_csr = H.off_pairs + words(size_t(P) * sizeof(int2));
+    H.off_csr_list = H.off_csr + words((nh + 1) * sizeof(int32_t));
+    const int32_t total = H.off_csr_list + words(std::max<size_t>(1, csr.size()) * sizeof(int32_t));
+    H.conf_indep = float(d->num_tors);
+    L.blob.assign(size_t(total), make_float4(0, 0, 0, 0));
+    char* base = reinterpret_cast<char*>(L.blob.data());
+    std::memcpy(base, &H, sizeof(H));
+    std::memcpy(base + 16 * size_t(H.off_atoms), atoms.data(), atoms.size() * sizeof(float4));
+    std::memcpy(base + 16 * size_t(H.off_nodes), nodes.data(), nodes.size() * sizeof(NodeRec));
+    if (P) std::memcpy(base + 16 * size_t(H.off_pairs), pairs.data(), pairs.size() * sizeof(int2));
+    std::memcpy(base + 16 * size_t(H.off_csr), csr_off.data(), csr_off.size() * sizeof(int32_t));
+    if (!csr.empty()) std::memcpy(base + 16 * size_t(H.off_csr_list), csr.data(), csr.size() * sizeof(int32_t));
+    L.heavy_index = heavy_index;
+    L.n_all_atoms = na;
+    L.num_tors = d->num_tors;
+    c.ligs.push_back(std::move(L));
+    c.pool_dirty = true;
+    *lig_id = int32_t(c.ligs.size()) - 1;
+    return VD_OK;
+}
+
+vd_status vd_ligand_info(vd_ctx* h, int32_t lig, int32_t* n_heavy, int32_t* ntors, int32_t* n_pairs) {
+    VD_CHECK(h && lig >= 0 && lig < int32_t(h->c.ligs.size()), VD_ERR_ARG, "vd_ligand_info: bad ligand id");
+    const LigHeader& H = h->c.ligs[lig].h;
+    if (n_heavy) *n_heavy = H.n_atoms;
+    if (ntors) *ntors = H.ntors;
+    if (n_pairs) *n_pairs = H.n_pairs;
+    return VD_OK;
+}
+
+vd_status vd_clear_ligands(vd_ctx* h) {
+    VD_CHECK(h, VD_ERR_ARG, "vd_clear_ligands: NULL context");
+    h->c.ligs.clear();
+    h->c.pool_dirty = true;
+    return VD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,249 @@
+// Warp-level local optimisation and Monte-Carlo moves (FP32).
+//
+// Vectors of the 6+ntors pose space are spread over the warp: component c
+// lives in lane c%32, slot c/32.  The pose (7+ntors floats) lives in shared
+// memory because the kinematics of every lane reads it.
+#pragma once
+
+#include <cfloat>
+
+#include "eval.cuh"
+
+namespace vd {
+
+constexpr float kPiF = 3.14159265358979f;
+
+// ---------------------------------------------------------------- Philox
+// Philox4x32-10 (Salmon et al., SC'11); the oracle uses the same streams.
+__host__ __device__ __forceinline__ void philox4x32(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                    uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = uint64_t(0xD2511F53u) * c0, p1 = uint64_t(0xCD9E8D57u) * c2;
+        const uint32_t hi0 = uint32_t(p0 >> 32), lo0 = uint32_t(p0), hi1 = uint32_t(p1 >> 32), lo1 = uint32_t(p1);
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+constexpr uint32_t kInitStep = 0xFFFFFFFFu;
+constexpr uint32_t kStreamTag = 0x5644u;
+__device__ __forceinline__ void draw(uint32_t seed, uint32_t lig, uint32_t chain, uint32_t step, uint32_t tag,
+                                     uint32_t u[4]) {
+    philox4x32(chain, step, tag, kStreamTag, seed, lig, u);
+}
+__device__ __forceinline__ float u01(uint32_t u) { return float(u >> 8) * (1.0f / 16777216.0f); }
+__device__ __forceinline__ float u01_open(uint32_t u) { return float((u >> 8) + 1) * (1.0f / 16777216.0f); }
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ float norm_angle(float x) {  // common.h:316-340
+    if (x > 3.f * kPiF) x -= 2.f * kPiF * ceilf((x - kPiF) / (2.f * kPiF));
+    else if (x < -3.f * kPiF) x += 2.f * kPiF * ceilf((-x - kPiF) / (2.f * kPiF));
+    if (x > kPiF) x -= 2.f * kPiF;
+    else if (x < -kPiF) x += 2.f * kPiF;
+    return x;
+}
+// q <- angle_to_quaternion(rot) * q, normalised (quaternion.cpp:235-240)
+__device__ __forceinline__ float4 quat_increment(float4 q, float r0, float r1, float r2) {
+    const float ang = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
+    if (ang > FLT_EPSILON) {
+        const float inv = 1.f / ang;
+        float s, c;
+        sincosf(0.5f * norm_angle(ang), &s, &c);
+        q = qmul(make_float4(c, s * r0 * inv, s * r1 * inv, s * r2 * inv), q);
+    }
+    const float n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    if (fabsf(n2 - 1.f) >= 1e-6f) {
+        const float inv = rsqrtf(n2);
+        q = make_float4(q.x * inv, q.y * inv, q.z * inv, q.w * inv);
+    }
+    return q;
+}
+
+struct Vec2 {  // one lane's share of a pose-space vector
+    float a, b;
+};
+__device__ __forceinline__ float vdot(Vec2 x, Vec2 y) { return warp_sum(x.a * y.a + x.b * y.b); }
+__device__ __forceinline__ Vec2 vload(const float* g, int n, int lane) {
+    Vec2 v;
+    v.a = (lane < n) ? g[lane] : 0.f;
+    v.b = (lane + 32 < n) ? g[lane + 32] : 0.f;
+    return v;
+}
+
+// x = xp + alpha * d (conf.h:367-372); xp, x in shared memory.
+__device__ __forceinline__ void conf_step(const float* xp, float* x, Vec2 d, float alpha, int nt, int lane) {
+    const float d0 = __shfl_sync(0xffffffffu, d.a, 0), d1 = __shfl_sync(0xffffffffu, d.a, 1),
+                d2 = __shfl_sync(0xffffffffu, d.a, 2), d3 = __shfl_sync(0xffffffffu, d.a, 3),
+                d4 = __shfl_sync(0xffffffffu, d.a, 4), d5 = __shfl_sync(0xffffffffu, d.a, 5);
+    if (lane == 0) {
+        x[0] = xp[0] + alpha * d0;
+        x[1] = xp[1] + alpha * d1;
+        x[2] = xp[2] + alpha * d2;
+        const float4 q = quat_increment(make_float4(xp[3], xp[4], xp[5], xp[6]), alpha * d3, alpha * d4, alpha * d5);
+        x[3] = q.x; x[4] = q.y; x[5] = q.z; x[6] = q.w;
+    }
+    const int t0 = lane - 6, t1 = lane + 26;  // torsion held in slot a / b
+    if (t0 >= 0 && t0 < nt) x[7 + t0] = norm_angle(xp[7 + t0] + norm_angle(alpha * d.a));
+    if (t1 < nt) x[7 + t1] = norm_angle(xp[7 + t1] + norm_angle(alpha * d.b));
+    __syncwarp();
+}
+
+__device__ __forceinline__ void copy_conf(const float* src, float* dst, int nc, int lane) {
+    for (int i = lane; i < nc; i += 32) dst[i] = src[i];
+    __syncwarp();
+}
+
+struct SearchMem {  // per-warp shared memory of the optimiser
+    WarpMem m;      // m.x is the working pose
+    float* xp;      // previous pose in the line search
+    float* xo;      // pose at entry (restored if the run got worse)
+};
+
+// quasi_newton.cuh:2172-2389 (RILC-BFGS) with the Lewis-Overton line search
+// of quasi_newton.cuh:1710-1806, on the pose in s.m.x.  Returns the energy;
+// s.m.x holds the optimised pose.  *evals counts energy+gradient calls.
+__device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const MapView& G, const float4* smooth,
+                           const EvalParams ep, int max_steps, int lane, int& evals) {
+    const int n = 6 + L.nt, nc = 7 + L.nt;
+    if (max_steps <= 0) max_steps = 1000;  // the reference's 0 means unbounded
+    float fx = eval_pose<true>(L, s.m, G, smooth, ep, lane);
+    ++evals;
+    Vec2 g = vload(s.m.g, n, lane);
+    const float fx_orig = fx;
+    copy_conf(s.m.x, s.xo, nc, lane);
+    Vec2 d = {-g.a, -g.b};
+    float gg = vdot(g, g);
+    if (!(sqrtf(gg) >= 1e-5f)) return fx;
+    float step = 1.f / sqrtf(vdot(d, d));
+    int k = 1;
+    for (;;) {
+        copy_conf(s.m.x, s.xp, nc, lane);
+        const Vec2 gp = g;
+        const float fxp = fx;
+        // ---- line search
+        int ls;
+        {
+            int count = 0;
+            bool brackt = false;
+            float mu = 0.f, nu = 1.0e20f;
+            const float dginit = vdot(gp, d);
+            if (0.f < dginit) {
+                ls = -1;
+            } else {
+                const float finit = fx, dgtest = 1.0e-4f * dginit, dstest = 0.1f * dginit;
+                for (;;) {
+                    conf_step(s.xp, s.m.x, d, step, L.nt, lane);
+                    fx = eval_pose<true>(L, s.m, G, smooth, ep, lane);
+                    ++evals;
+                    g = vload(s.m.g, n, lane);
+                    ++count;
+                    if (fx > finit + step * dgtest) {
+                        nu = step;
+                        brackt = true;
+                    } else {
+                        if (vdot(g, d) < dstest) mu = step;
+                        else { ls = count; break; }
+                    }
+                    if (count >= 10) { ls = (fx > finit) ? -1 : count; break; }
+                    step = brackt ? 0.5f * (mu + nu) : 2.f * step;
+                }
+            }
+        }
+        if (ls < 0) {
+            copy_conf(s.xp, s.m.x, nc, lane);
+            g = gp;
+            fx = fxp;
+            break;
+        }
+        if (!(sqrtf(vdot(g, g)) >= 1e-5f)) return fx;
+        if (max_steps <= k) break;
+        ++k;
+        const Vec2 sv = {step * d.a, step * d.b};
+        const Vec2 yv = {g.a - gp.a, g.b - gp.b};
+        const float ys = vdot(yv, sv), yy = vdot(yv, yv);
+        d = {-g.a, -g.b};
+        const float cau = vdot(sv, sv) * sqrtf(vdot(gp, gp)) * 1.0e-6f;
+        if (ys > cau) {
+            const float alpha = vdot(sv, d) / ys;
+            d.a += alpha * yv.a; d.b += alpha * yv.b;
+            const float sc = ys / yy;
+            d.a *= sc; d.b *= sc;
+            const float beta = vdot(yv, d) / ys;
+            d.a += (alpha - beta) * sv.a; d.b += (alpha - beta) * sv.b;
+        }
+        step = 1.f;
+    }
+    if (!(fx <= fx_orig)) {
+        fx = fx_orig;
+        copy_conf(s.xo, s.m.x, nc, lane);
+    }
+    return fx;
+}
+
+// Random initial pose (conf.h:137-140 rigid_conf::randomize, torsions in
+// [-pi, pi]) from the chain's Philox stream; written to x.
+__device__ __forceinline__ void init_pose(float* x, int nt, uint32_t seed, uint32_t lig, uint32_t chain,
+                                          const float lo[3], const float hi[3], int lane) {
+    uint32_t u[4], q[4];
+    draw(seed, lig, chain, kInitStep, 0, u);
+    draw(seed, lig, chain, kInitStep, 1, q);
+    if (lane == 0) {
+        for (int i = 0; i < 3; ++i) x[i] = lo[i] + u01(u[i]) * (hi[i] - lo[i]);
+        const float r0 = sqrtf(-2.f * logf(u01_open(q[0]))), r1 = sqrtf(-2.f * logf(u01_open(q[2])));
+        float s0, c0, s1, c1;
+        sincosf(2.f * kPiF * u01(q[1]), &s0, &c0);
+        sincosf(2.f * kPiF * u01(q[3]), &s1, &c1);
+        float n4[4] = {r0 * c0, r0 * s0, r1 * c1, r1 * s1};
+        float nrm = sqrtf(n4[0] * n4[0] + n4[1] * n4[1] + n4[2] * n4[2] + n4[3] * n4[3]);
+        if (!(nrm > 1e-6f)) { n4[0] = 1.f; n4[1] = n4[2] = n4[3] = 0.f; nrm = 1.f; }
+        for (int i = 0; i < 4; ++i) x[3 + i] = n4[i] / nrm;
+    }
+    for (int t = lane; t < nt; t += 32) {
+        uint32_t v[4];
+        draw(seed, lig, chain, kInitStep, 2 + t / 4, v);
+        x[7 + t] = -kPiF + 2.f * kPiF * u01(v[t & 3]);
+    }
+    __syncwarp();
+}
+
+// mutate.cpp:62-127: one of position (2 A ball), orientation (2/Rg ball,
+// Rg = heavy-atom gyration radius about the root origin, model.cpp:1161),
+// or one torsion set uniformly in [-pi, pi].
+__device__ __forceinline__ void mutate_pose(const LigView& L, const WarpMem& m, uint32_t seed, uint32_t lig,
+                                            uint32_t chain, uint32_t step, float amplitude, int lane) {
+    uint32_t a[4], b[4];
+    draw(seed, lig, chain, step, 0, a);
+    draw(seed, lig, chain, step, 1, b);
+    const int mm = 2 + L.nt;
+    int which = int(u01(a[0]) * float(mm));
+    if (which > mm - 1) which = mm - 1;
+    const float z = 2.f * u01(a[1]) - 1.f, phi = 2.f * kPiF * u01(a[2]), r = cbrtf(u01(a[3]));
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    const float sz = sqrtf(fmaxf(0.f, 1.f - z * z));
+    const float s0 = r * sz * cp, s1 = r * sz * sp, s2 = r * z;
+    if (which == 0) {
+        if (lane == 0) { m.x[0] += amplitude * s0; m.x[1] += amplitude * s1; m.x[2] += amplitude * s2; }
+    } else if (which == 1) {
+        kinematics(L, m, lane);
+        float acc = 0.f;
+        for (int i = lane; i < L.na; i += 32) {
+            const float dx = m.cx[i] - m.x[0], dy = m.cy[i] - m.x[1], dz = m.cz[i] - m.x[2];
+            acc += dx * dx + dy * dy + dz * dz;
+        }
+        acc = warp_sum(acc);
+        const float gr = sqrtf(acc / float(L.na));
+        if (gr > FLT_EPSILON && lane == 0) {
+            const float f = amplitude / gr;
+            const float4 q = quat_increment(make_float4(m.x[3], m.x[4], m.x[5], m.x[6]), f * s0, f * s1, f * s2);
+            m.x[3] = q.x; m.x[4] = q.y; m.x[5] = q.z; m.x[6] = q.w;
+        }
+    } else {
+        if (lane == 0) m.x[7 + which - 2] = -kPiF + 2.f * kPiF * u01(b[0]);
+    }
+    __syncwarp();
+}
+
+}  // namespace vd
