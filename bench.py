@@ -1,0 +1,316 @@
+#!/usr/bin/env python
+"""Benchmark: wide-box virtual screen through the batched + adjoint docking path.
+
+Workload (synthetic stand-in for the reference's screening sets): an 8,000
+heavy-atom receptor (uniform in a 60 A-radius ball, >= 2.8 A separation),
+a 70x70x70 A box at 0.375 A (188^3 points x 8 XS maps, built once and
+reported separately), and ligands of 15-45 heavy atoms / 2-12 torsions,
+each docked with 6,500 Monte-Carlo chains (RILC-BFGS local search, heuristic
+search depth) followed by GPU clustering, refinement and rescoring of its
+top 20 poses.  One step = one batch of ligands through vd_dock_batched (one
+persistent launch over all (ligand, chain) items).  The plain form
+(vd_dock_plain, one ligand per launch) is timed on a sample beside it.
+
+Run: python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Under torchrun each rank docks its own ligand batches (weak scaling, no
+data-path collective); time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "vina-cuda_b200"))
+
+METRIC = "ligands/s (batched + adjoint docking, wide-box screen)"
+UNIT = "ligands/s"
+BOX = 70.0
+REC_ATOMS, REC_RADIUS = 8000, 60.0
+LIG_ATOMS, LIG_TORS = (15, 45), (2, 12)
+CHAINS = 6500
+SEED = 20261203
+
+
+def args_():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=8)
+    a.add_argument("--warmup", type=int, default=3)
+    a.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    a.add_argument("--batch", type=int, default=64, help="ligands per step")
+    a.add_argument("--chains", type=int, default=CHAINS)
+    a.add_argument("--plain-ligands", type=int, default=8)
+    a.add_argument("--e2e-steps", type=int, default=2)
+    a.add_argument("--no-cpu-baseline", action="store_true")
+    a.add_argument("--cpu-ligands", type=int, default=3, help="whole ligands in the CPU sample")
+    return a.parse_args()
+
+
+def dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(rank, n_ligs):
+    from vdock import synth
+    xyz, xs = synth.receptor(REC_ATOMS, REC_RADIUS, SEED)
+    ligs = synth.ligand_set(n_ligs, LIG_ATOMS, LIG_TORS, SEED + 7919 * (rank + 1))
+    return xyz, xs, ligs
+
+
+def lig_bytes(lig):
+    """Algorithmic bytes of one BFGS evaluation: 8 FP32 grid corners per
+    heavy atom and two (e, dE/dr) table entries per intra pair."""
+    heavy = int((lig["xs"] >= 0).sum())
+    return 32 * heavy + 16 * len(lig["pairs"])
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(xyz, xs, ligs, chains_per_lig, n_sample):
+    """Oracle port (double precision restatement of the reference's search,
+    clustering and refinement) timed on the host cores on a bounded sample
+    of the same workload: n_sample whole ligands (all chains, top-20
+    refinement)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+    import oracle_lib
+    from vdock import synth
+    threads = os.cpu_count() or 1
+    orc = oracle_lib.Oracle()
+    orc.set_receptor(xyz, xs)
+    orc.set_box([0, 0, 0], [BOX] * 3)
+    t_grid = orc.grid_seconds(synth.TYPES8, threads)
+    total_t, total_evals, desc = 0.0, 0, []
+    for lig in ligs[:n_sample]:
+        lo = orc.add_ligand(lig)
+        n_all, nt = lig["n_atoms"], orc.ntors[lo]
+        depth = max(1, int((0.24 * n_all + 0.29 * nt - 3.41) * 2))
+        steps = (30 + n_all) // 3
+        t0 = time.perf_counter()
+        conf, e, evals = orc.mc_chains(lo, SEED, lo, depth, steps, 0, chains_per_lig, threads=threads)
+        kept = orc.cluster(lo, conf, e, 1.0, 20)
+        for i in kept:
+            _, _, ev = orc.refine(lo, conf[i], steps)
+            evals += ev
+        total_t += time.perf_counter() - t0
+        total_evals += evals
+        desc.append(f"{n_all}/{nt}")
+    return {"value": len(desc) / total_t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(desc)} whole ligands (atoms/torsions {', '.join(desc)}), {chains_per_lig} chains "
+                      f"each, heuristic depth, top-20 refinement; {total_evals} BFGS evals in {total_t:.1f} s",
+            "grid_build_s": t_grid, "bfgs_evals_per_s": total_evals / total_t}
+
+
+def run_reference(a):
+    world, rank, _ = dist()
+    if rank != 0:
+        return
+    xyz, xs, ligs = make_inputs(0, a.cpu_ligands)
+    t0 = time.perf_counter()
+    cb = cpu_baseline(xyz, xs, ligs, a.chains, a.cpu_ligands)
+    wall = time.perf_counter() - t0
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 * a.batch / cb["value"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "wide-box screen", "ligands_per_step": a.batch, "chains_per_ligand": a.chains,
+                       "box_A": BOX, "receptor_atoms": REC_ATOMS},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+    import vdock
+    from vdock import synth
+    world, rank, local = dist()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = td
+    B, W, K = a.batch, a.warmup, a.steps
+    n_ligs = (W + K) * B + a.plain_ligands
+    xyz, xs, ligs = make_inputs(rank, n_ligs)
+    ctx = vdock.Context(local)
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0, 0, 0], [BOX] * 3)
+    grid_ms = []
+    for _ in range(3):
+        ctx.build_grids(synth.TYPES8)
+        grid_ms.append(ctx.stats()["grid_ms"])
+    n_pts = int(np.prod(ctx.grid_dims()[0]))
+    grid_bytes = 4 * n_pts * 8 + 16 * REC_ATOMS
+    ids = [ctx.add_ligand(l) for l in ligs]
+    sp = vdock.search_params(seed=SEED, n_chains=a.chains, search_depth=0, refine=1)
+    batches = [ids[i * B:(i + 1) * B] for i in range(W + K)]
+    for k in range(W):
+        ctx.dock_batched(batches[k], sp)
+    torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    dock_ms, evals, abytes, launches = 0.0, 0, 0, 0
+    t_wall = time.perf_counter()
+    for k in range(W, W + K):
+        res = ctx.dock_batched(batches[k], sp)
+        st = ctx.stats()
+        dock_ms += st["dock_ms"]
+        for lid, r in zip(batches[k], res):
+            evals += r["bfgs_evals"]
+            abytes += r["bfgs_evals"] * lig_bytes(ligs[lid])
+        launches += 5  # dock, cluster, gather, refine, score
+    ev1.record()
+    torch.cuda.synchronize()
+    t_wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    if pg:
+        t = torch.tensor([elapsed], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        elapsed = float(t.item())
+        pg.barrier()
+    value = K * B * world / elapsed
+    # plain form on a sample (one ligand per launch)
+    plain_ids = ids[(W + K) * B:]
+    ctx.dock_plain(plain_ids[0], sp)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for lid in plain_ids:
+        ctx.dock_plain(lid, sp)
+    torch.cuda.synchronize()
+    plain_value = len(plain_ids) / (time.perf_counter() - t0)
+    # end to end through the public API with host buffers: ligand topologies
+    # copied in (vd_add_ligand + pool upload), results read back
+    e2e_times, h2d, d2h = [], 0, 0
+    for k in range(min(a.e2e_steps, K)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.clear_ligands()
+        eids = [ctx.add_ligand(ligs[lid]) for lid in batches[W + k]]
+        res = ctx.dock_batched(eids, sp)
+        torch.cuda.synchronize()
+        e2e_times.append(time.perf_counter() - t0)
+    blob_bytes = sum(64 + 16 * int((l["xs"] >= 0).sum()) + 48 * len(l["node_parent"]) + 16 * len(l["pairs"]) +
+                     4 * int((l["xs"] >= 0).sum()) for l in (ligs[i] for i in batches[W]))
+    h2d = blob_bytes
+    d2h = B * 2 * 1024  # vd_dock_result per ligand
+    e2e_value = B * world / statistics.median(e2e_times) if e2e_times else None
+    if rank != 0:
+        return
+    hbm, src = peaks()
+    achieved = abytes / (dock_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * elapsed / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "wide-box screen", "ligands_per_step": B, "chains_per_ligand": a.chains,
+                   "search_depth": "heuristic (main.cpp:369)", "box_A": BOX, "receptor_atoms": REC_ATOMS,
+                   "ligand_atoms": list(LIG_ATOMS), "ligand_torsions": list(LIG_TORS),
+                   "parallelism": f"weak x{world} (ligand shards)",
+                   "l2": "inputs larger than L2 (8 maps x 188^3 x 4 B = 213 MB)"},
+        "bfgs_evals_per_s": evals * world / elapsed,
+        "plain": {"value": plain_value * world, "unit": UNIT, "ligands": len(plain_ids),
+                  "batched_over_plain": value / (plain_value * world)},
+        "grid_build": {"ms": min(grid_ms), "points": n_pts, "types": 8,
+                       "gbs": grid_bytes / (min(grid_ms) / 1e3) / 1e9,
+                       "frac_of_hbm": grid_bytes / (min(grid_ms) / 1e3) / 1e9 / hbm},
+        "roofline": {"kernel": "dock_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
+                     "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+                     "note": "algorithmic bytes = evals x (32 x heavy atoms + 16 x intra pairs)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "wall_s": t_wall,
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        cb = cpu_baseline(xyz, xs, ligs, a.chains, a.cpu_ligands)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line["grid_build"]["cpu_s"] = cb["grid_build_s"]
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as td
+        if td.is_initialized():
+            td.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

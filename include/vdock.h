@@ -95,7 +95,8 @@ typedef struct {
     float   rmsd_lb[VD_MAX_MODES];         /* to mode 1 (model.cpp:1485-1507)    */
     float   rmsd_ub[VD_MAX_MODES];
     float   pose[VD_MAX_MODES][7 + VD_MAX_TORS];
-    int64_t bfgs_evals;                    /* energy+gradient evaluations        */
+    int64_t bfgs_evals;                    /* Monte-Carlo search energy+gradient
+                                              evaluations of this ligand         */
 } vd_dock_result;
 
 typedef struct {

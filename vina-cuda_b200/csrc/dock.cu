@@ -38,6 +38,7 @@ struct DockParams {
     float* out_e;                // [items]
     int32_t* queue;
     unsigned long long* evals;
+    unsigned long long* lig_evals;  // [n_ligs] evaluations per ligand
     int32_t warp_floats;
     int32_t warps_per_block;
 };
@@ -78,6 +79,7 @@ __global__ void __launch_bounds__(256) dock_kernel(DockParams p) {
         float* xb = xt + nc4;        // chain best
         const uint32_t uid = __ldg(&p.lig_uid[li]);
         const int depth = __ldg(&p.depth[li]), steps = __ldg(&p.bfgs_steps[li]);
+        const int evals0 = evals;
         init_pose(xt, L.nt, p.seed, uid, chain, p.lo, p.hi, lane);
         copy_conf(xt, xb, nc, lane);
         float tmp_e = FLT_MAX, best_e = INFINITY;
@@ -103,7 +105,10 @@ __global__ void __launch_bounds__(256) dock_kernel(DockParams p) {
         }
         float* dst = p.out_conf + size_t(item) * p.stride;
         for (int i = lane; i < nc; i += 32) dst[i] = xb[i];
-        if (lane == 0) p.out_e[item] = best_e;
+        if (lane == 0) {
+            p.out_e[item] = best_e;
+            atomicAdd(&p.lig_evals[li], (unsigned long long)(evals - evals0));
+        }
         __syncwarp();
         if (!persistent) break;
     }
@@ -159,7 +164,8 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
     const size_t b_off = n * sizeof(int64_t), b_pre = (n + 1) * sizeof(int32_t), b_arr = n * sizeof(int32_t);
     const size_t b_conf = size_t(items) * out.stride * sizeof(float), b_e = size_t(items) * sizeof(float);
     auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
-    const size_t total = al(b_off) + al(b_pre) + 3 * al(b_arr) + al(b_conf) + al(b_e) + out.extra_bytes;
+    const size_t b_lev = n * sizeof(unsigned long long);
+    const size_t total = al(b_off) + al(b_pre) + 3 * al(b_arr) + al(b_conf) + al(b_e) + al(b_lev) + out.extra_bytes;
     st = ensure_scratch(&c, total);
     if (st != VD_OK) return st;
     char* s = static_cast<char*>(c.d_scratch);
@@ -170,7 +176,9 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
     int32_t* d_steps = reinterpret_cast<int32_t*>(s); s += al(b_arr);
     out.d_conf = reinterpret_cast<float*>(s); s += al(b_conf);
     out.d_e = reinterpret_cast<float*>(s); s += al(b_e);
+    out.d_lig_evals = reinterpret_cast<unsigned long long*>(s); s += al(b_lev);
     out.d_extra = s;
+    VD_CUDA(cudaMemsetAsync(out.d_lig_evals, 0, b_lev, stream));
     VD_CUDA(cudaMemcpyAsync(d_off, off.data(), b_off, cudaMemcpyHostToDevice, stream));
     VD_CUDA(cudaMemcpyAsync(d_pre, prefix.data(), b_pre, cudaMemcpyHostToDevice, stream));
     VD_CUDA(cudaMemcpyAsync(d_uid, uid.data(), b_arr, cudaMemcpyHostToDevice, stream));
@@ -199,6 +207,7 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
     p.out_e = out.d_e;
     p.queue = c.d_counter;
     p.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 2);
+    p.lig_evals = out.d_lig_evals;
     p.warp_floats = max_wf;
     // launch shape: warps per block from the override / autotuner, as many
     // resident blocks as fit for the persistent form

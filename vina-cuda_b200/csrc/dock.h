@@ -13,6 +13,7 @@ struct DockBuffers {
     std::vector<int32_t> prefix;    // first item of each ligand (host)
     float* d_conf = nullptr;        // [items][stride] chain best poses
     float* d_e = nullptr;           // [items] chain best energies
+    unsigned long long* d_lig_evals = nullptr;  // [n_ligs] evaluations per ligand
     size_t extra_bytes = 0;         // caller-requested scratch after the outputs
     char* d_extra = nullptr;
 };

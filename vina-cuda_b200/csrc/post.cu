@@ -834,15 +834,16 @@ vd_status dock_pipeline(Ctx& c, const std::vector<int>& ligs, const vd_search_pa
     st = post_process(c, ligs, sp, db, out, c.stream);
     if (st != VD_OK) return st;
     unsigned long long ev[2] = {0, 0};
+    std::vector<unsigned long long> lev(ligs.size());
     VD_CUDA(cudaMemcpyAsync(ev, c.d_counter + 2, 16, cudaMemcpyDeviceToHost, c.stream));
+    VD_CUDA(cudaMemcpyAsync(lev.data(), db.d_lig_evals, lev.size() * 8, cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaStreamSynchronize(c.stream));
     float post_ms = 0;
     VD_CUDA(cudaEventElapsedTime(&post_ms, c.ev0, c.ev1));
     c.stats.dock_ms = dock_ms;
     c.stats.post_ms = post_ms;
     c.stats.bfgs_evals += int64_t(ev[0] + ev[1]);
-    // chain evaluations per ligand are not separated; report the batch total on the first result
-    for (size_t i = 0; i < ligs.size(); ++i) out[i].bfgs_evals = (i == 0) ? int64_t(ev[0] + ev[1]) : 0;
+    for (size_t i = 0; i < ligs.size(); ++i) out[i].bfgs_evals = int64_t(lev[i]);  // search evaluations
     return VD_OK;
 }
 
