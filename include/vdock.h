@@ -144,6 +144,8 @@ vd_status vd_energy_grad(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const flo
 vd_status vd_energy_grad_device(vd_ctx* ctx, int32_t lig_id, int32_t n_poses,
                                 const float* poses_device, const vd_eval_params* p,
                                 float* e_device, float* g_device, void* stream);
+vd_status vd_energy_device(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses_device,
+                           const vd_eval_params* p, float* e_device, void* stream);
 /* Heavy-atom coordinates of poses (forward kinematics only): [n][n_heavy][3]. */
 vd_status vd_pose_coords(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
                          float* xyz_out);

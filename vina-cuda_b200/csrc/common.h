@@ -46,8 +46,7 @@ void set_error(const std::string& msg);
 
 // ---------------------------------------------------------------- device ligand
 // One ligand is one contiguous blob of 16-byte words in the ligand pool:
-//   LigHeader | atoms (float4) | nodes (NodeRec) | pairs (int2) |
-//   csr offsets (int, n_heavy+1, padded) | csr entries (int, padded)
+//   LigHeader | atoms (float4) | nodes (NodeRec) | pairs (int2)
 // Only heavy atoms (XS type >= 0) are on the device; hydrogens carry no
 // energy and are placed on the host when output files are written.
 struct LigHeader {
@@ -58,18 +57,15 @@ struct LigHeader {
     int32_t off_atoms;    // in 16-byte words from the blob start
     int32_t off_nodes;
     int32_t off_pairs;    // int2 entries start (16-byte word offset)
-    int32_t off_csr;      // int entries start (16-byte word offset)
-    int32_t off_csr_list;
     int32_t max_depth;
-    int32_t n_csr;        // 2*n_pairs
-    int32_t pad0;
-    float conf_indep;     // 1 / (1 + w*num_tors/5)
-    float pad1, pad2, pad3;
+    int32_t pad0, pad1, pad2, pad6;
+    float num_tors;       // N_tors of the conf-independent term
+    float pad3, pad4, pad5;
 };
 static_assert(sizeof(LigHeader) == 64, "header size");
 
 // Atom word: local coords (relative to its rigid body's origin) and
-// (xs type | node << 8) stored in .w as int bits.
+// (xs type | node << 8 | element << 16) stored in .w as int bits.
 // Rigid body record: origin relative to parent frame, torsion axis in the
 // parent frame, parent index, atom range and subtree end (pre-order).
 struct NodeRec {

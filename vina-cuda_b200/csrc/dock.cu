@@ -54,7 +54,10 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
 }
 
 template <bool persistent>
-__global__ void __launch_bounds__(256) dock_kernel(DockParams p) {
+#ifndef VD_DOCK_MIN_BLOCKS
+#define VD_DOCK_MIN_BLOCKS 8  // 4-warp blocks per SM the register budget targets
+#endif
+__global__ void __launch_bounds__(128, VD_DOCK_MIN_BLOCKS) dock_kernel(DockParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* base = reinterpret_cast<float*>(smem4) + size_t(wid) * p.warp_floats;
@@ -86,21 +89,29 @@ __global__ void __launch_bounds__(256) dock_kernel(DockParams p) {
         for (int step = 0; step < depth; ++step) {
             copy_conf(xt, s.m.x, nc, lane);
             mutate_pose(L, s.m, p.seed, uid, chain, uint32_t(step), p.amplitude, lane);
-            const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
             uint32_t b[4];
             draw(p.seed, uid, chain, uint32_t(step), 1, b);
-            const bool accept =
-                step == 0 || ce < tmp_e || u01(b[1]) < expf((tmp_e - ce) / p.temperature);  // kernel2.cu:63-71
-            if (accept) {
-                tmp_e = ce;
-                if (tmp_e < best_e) {
-                    tmp_e = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
+            // pass 0 optimises the candidate; pass 1 re-optimises an accepted
+            // candidate that beats the chain's best (one optimiser call site)
+            for (int pass = 0; pass < 2; ++pass) {
+                const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
+                if (pass == 0) {
+                    const bool accept = step == 0 || ce < tmp_e ||
+                                        u01(b[1]) < __expf((tmp_e - ce) / p.temperature);  // kernel2.cu:63-71
+                    if (!accept) break;
+                    tmp_e = ce;
+                    if (!(tmp_e < best_e)) {
+                        copy_conf(s.m.x, xt, nc, lane);
+                        break;
+                    }
+                } else {
+                    tmp_e = ce;
                     if (tmp_e < best_e) {
                         best_e = tmp_e;
                         copy_conf(s.m.x, xb, nc, lane);
                     }
+                    copy_conf(s.m.x, xt, nc, lane);
                 }
-                copy_conf(s.m.x, xt, nc, lane);
             }
         }
         float* dst = p.out_conf + size_t(item) * p.stride;

@@ -6,14 +6,17 @@
 //        q_k = q_root * aa_j1 * ... * aa_k,  o_k = o_root + R_root * w_k
 //      (rotation about a body-fixed axis; equals tree.h:282-292)
 //   3. lanes = atoms: coordinates, trilinear grid term (grid.cpp:50-160)
-//   4. lanes = pairs: intra pair term and pair force (model.cpp:1241-1256)
-//   5. lanes = atoms: per-atom force = grid gradient + incident pair forces
+//   4. lanes = segments of the pair list sorted by second atom: intra pair
+//      term; the force on the second atom is accumulated in registers and
+//      the force on the first atom is added with a shared-memory atomic
+//      (model.cpp:1241-1256)
 //   6. lanes = bodies: own force and moment about the root origin
 //   7. lanes = bodies: subtree sums over the pre-order range [k, end_k),
 //        torque T_k = M_k - (o_k - o_root) x F_k, dE/dtorsion = T_k . axis_k
 //      (the bottom-up recursion of tree.h:169-178, 341-348, 373-422)
 //   8. warp butterfly sum of the energy (deterministic).
-// All sums run in a fixed order, so results are bit-reproducible.
+// The per-body and subtree sums run in a fixed order; the pair-force
+// atomics are issued in a fixed program order by a single warp.
 #pragma once
 
 #include "common.h"
@@ -35,8 +38,6 @@ struct LigView {
     const float4* atoms;
     const NodeRec* nodes;
     const int2* pairs;
-    const int32_t* csr_off;
-    const int32_t* csr;
     int32_t na, nn, np, nt;
     float num_tors;
 };
@@ -49,29 +50,30 @@ __device__ __forceinline__ LigView lig_view(const float4* pool, int64_t off) {
     L.nn = h->n_nodes;
     L.np = h->n_pairs;
     L.nt = h->ntors;
-    L.num_tors = h->conf_indep;
+    L.num_tors = h->num_tors;
     L.atoms = b + h->off_atoms;
     L.nodes = reinterpret_cast<const NodeRec*>(b + h->off_nodes);
     L.pairs = reinterpret_cast<const int2*>(b + h->off_pairs);
-    L.csr_off = reinterpret_cast<const int32_t*>(b + h->off_csr);
-    L.csr = reinterpret_cast<const int32_t*>(b + h->off_csr_list);
     return L;
 }
 
-constexpr int kNodeF = 20;  // q[4], o[3], R[9], aa[4]
+// Body frame in shared memory, 20 floats: three rows [R(i,0) R(i,1) R(i,2) o_i]
+// (so an atom position is three 128-bit loads), the quaternion and the
+// local rotation about the body's torsion axis.
+constexpr int kNodeF = 20;
+constexpr int kNdQ = 12, kNdAA = 16;
 
 __host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
 // Shared-memory floats one warp needs for a ligand of the given size.
 __host__ __device__ inline int warp_floats(int na, int nn, int np, int nt) {
-    return pad4(7 + nt) + kNodeF * nn + 6 * pad4(na) + 3 * pad4(np) + pad4(6 * nn) + pad4(6 + nt);
+    return pad4(7 + nt) + kNodeF * nn + 4 * na + 3 * pad4(na) + pad4(6 * nn) + pad4(6 + nt);
 }
 
 struct WarpMem {
     float* x;
     float* nd;
-    float *cx, *cy, *cz;
+    float4* c;          // heavy-atom coordinates (w unused)
     float *fx, *fy, *fz;
-    float *px, *py, *pz;
     float* ns;
     float* g;
 };
@@ -80,16 +82,11 @@ __device__ __forceinline__ WarpMem carve(float* p, int na, int nn, int np, int n
     WarpMem m;
     m.x = p; p += pad4(7 + nt);
     m.nd = p; p += kNodeF * nn;
-    const int a4 = pad4(na), p4 = pad4(np);
-    m.cx = p; p += a4;
-    m.cy = p; p += a4;
-    m.cz = p; p += a4;
+    const int a4 = pad4(na);
+    m.c = reinterpret_cast<float4*>(p); p += 4 * na;
     m.fx = p; p += a4;
     m.fy = p; p += a4;
     m.fz = p; p += a4;
-    m.px = p; p += p4;
-    m.py = p; p += p4;
-    m.pz = p; p += p4;
     m.ns = p; p += pad4(6 * nn);
     m.g = p;
     return m;
@@ -116,20 +113,21 @@ __device__ __forceinline__ float3 qrot(float4 q, float3 v) {
     return make_float3(v.x + 2.f * (q.z * tz - q.w * ty), v.y + 2.f * (q.w * tx - q.y * tz),
                        v.z + 2.f * (q.y * ty - q.z * tx));
 }
-// quaternion.cpp:155-192 layout: R[i + 3j] = row i, column j.
-__device__ __forceinline__ void qmat(float4 q, float* R) {
+// Rotation matrix of a unit quaternion (quaternion.cpp:155-192), written as
+// the rows of the body frame: nd[4*i + j] = R(i, j).
+__device__ __forceinline__ void qmat_rows(float4 q, float* nd) {
     const float a = q.x, b = q.y, c = q.z, d = q.w;
     const float aa = a * a, ab = a * b, ac = a * c, ad = a * d, bb = b * b, bc = b * c, bd = b * d,
                 cc = c * c, cd = c * d, dd = d * d;
-    R[0] = aa + bb - cc - dd;
-    R[3] = 2.f * (-ad + bc);
-    R[6] = 2.f * (ac + bd);
-    R[1] = 2.f * (ad + bc);
-    R[4] = aa - bb + cc - dd;
-    R[7] = 2.f * (-ab + cd);
-    R[2] = 2.f * (-ac + bd);
-    R[5] = 2.f * (ab + cd);
-    R[8] = aa - bb - cc + dd;
+    nd[0] = aa + bb - cc - dd;
+    nd[1] = 2.f * (-ad + bc);
+    nd[2] = 2.f * (ac + bd);
+    nd[4] = 2.f * (ad + bc);
+    nd[5] = aa - bb + cc - dd;
+    nd[6] = 2.f * (-ab + cd);
+    nd[8] = 2.f * (-ac + bd);
+    nd[9] = 2.f * (ab + cd);
+    nd[10] = aa - bb - cc + dd;
 }
 
 // Phases 1-3a: rigid-body frames and heavy-atom coordinates from the pose in m.x.
@@ -139,12 +137,11 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
         float4 aa = make_float4(1.f, 0.f, 0.f, 0.f);
         if (k > 0) {
             float s, c;
-            sincosf(0.5f * m.x[7 + k - 1], &s, &c);
+            __sincosf(0.5f * m.x[7 + k - 1], &s, &c);  // |angle| <= pi/2, abs error < 1e-6
             const NodeRec& n = L.nodes[k];
             aa = make_float4(c, s * __ldg(&n.axis[0]), s * __ldg(&n.axis[1]), s * __ldg(&n.axis[2]));
         }
-        float* nd = m.nd + kNodeF * k;
-        nd[16] = aa.x; nd[17] = aa.y; nd[18] = aa.z; nd[19] = aa.w;
+        *reinterpret_cast<float4*>(m.nd + kNodeF * k + kNdAA) = aa;
     }
     __syncwarp();
     // 2: frames by walking the ancestor path
@@ -154,14 +151,12 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
         float4 P = make_float4(1.f, 0.f, 0.f, 0.f);
         float3 w = make_float3(0.f, 0.f, 0.f);
         if (k > 0) {
-            const float* ndk = m.nd + kNodeF * k;
-            P = make_float4(ndk[16], ndk[17], ndk[18], ndk[19]);
+            P = *reinterpret_cast<const float4*>(m.nd + kNodeF * k + kNdAA);
             const NodeRec& nk = L.nodes[k];
             w = make_float3(__ldg(&nk.rel_origin[0]), __ldg(&nk.rel_origin[1]), __ldg(&nk.rel_origin[2]));
             int j = __ldg(&nk.parent);
             while (j > 0) {
-                const float* ndj = m.nd + kNodeF * j;
-                const float4 aj = make_float4(ndj[16], ndj[17], ndj[18], ndj[19]);
+                const float4 aj = *reinterpret_cast<const float4*>(m.nd + kNodeF * j + kNdAA);
                 const NodeRec& nj = L.nodes[j];
                 const float3 r = qrot(aj, w);
                 w = make_float3(__ldg(&nj.rel_origin[0]) + r.x, __ldg(&nj.rel_origin[1]) + r.y,
@@ -175,20 +170,20 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
         q = make_float4(q.x * inv, q.y * inv, q.z * inv, q.w * inv);
         const float3 ro = qrot(qr, w);
         float* nd = m.nd + kNodeF * k;
-        nd[0] = q.x; nd[1] = q.y; nd[2] = q.z; nd[3] = q.w;
-        nd[4] = orr.x + ro.x; nd[5] = orr.y + ro.y; nd[6] = orr.z + ro.z;
-        qmat(q, nd + 7);
+        *reinterpret_cast<float4*>(nd + kNdQ) = q;
+        nd[3] = orr.x + ro.x; nd[7] = orr.y + ro.y; nd[11] = orr.z + ro.z;
+        qmat_rows(q, nd);
     }
     __syncwarp();
     // 3a: heavy-atom coordinates
     for (int i = lane; i < L.na; i += 32) {
         const float4 a = __ldg(&L.atoms[i]);
         const int k = (__float_as_int(a.w) >> 8) & 0xff;
-        const float* nd = m.nd + kNodeF * k;
-        const float* R = nd + 7;
-        m.cx[i] = nd[4] + (R[0] * a.x + R[3] * a.y + R[6] * a.z);
-        m.cy[i] = nd[5] + (R[1] * a.x + R[4] * a.y + R[7] * a.z);
-        m.cz[i] = nd[6] + (R[2] * a.x + R[5] * a.y + R[8] * a.z);
+        const float4* nd = reinterpret_cast<const float4*>(m.nd + kNodeF * k);
+        const float4 r0 = nd[0], r1 = nd[1], r2 = nd[2];
+        m.c[i] = make_float4(r0.w + (r0.x * a.x + r0.y * a.y + r0.z * a.z),
+                             r1.w + (r1.x * a.x + r1.y * a.y + r1.z * a.z),
+                             r2.w + (r2.x * a.x + r2.y * a.y + r2.z * a.z), 0.f);
     }
     __syncwarp();
 }
@@ -225,7 +220,7 @@ __device__ __forceinline__ float grid_term(const MapView& G, const float* map, f
     float yg = (f010 - f000) * mx * mz + (f110 - f100) * x * mz + (f011 - f001) * mx * z + (f111 - f101) * x * z;
     float zg = (f001 - f000) * mx * my + (f101 - f100) * x * my + (f011 - f010) * mx * y + (f111 - f110) * x * y;
     if (f > 0.f) {  // curl (curl.h:31-40)
-        const float t = v / (v + f);
+        const float t = __fdividef(v, v + f);
         f *= t;
         const float t2 = t * t;
         xg *= t2; yg *= t2; zg *= t2;
@@ -245,7 +240,7 @@ __device__ __forceinline__ float pair_term(const float4* smooth, int tp, float r
     float e = t.x + rem * (t.z - t.x);
     dor = t.y + rem * (t.w - t.y);
     if (e > 0.f) {
-        const float c = v / (v + e);
+        const float c = __fdividef(v, v + e);
         e *= c;
         dor *= c * c;
     }
@@ -269,66 +264,91 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
                              float v_intra, int lane) {
     kinematics(L, m, lane);
     float e = 0.f;
-    // 3b: grid term per atom
-    float gxs[4], gys[4], gzs[4];
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const int i = lane + 32 * s;
-        gxs[s] = gys[s] = gzs[s] = 0.f;
-        if (i < L.na) {
-            const int t = __float_as_int(__ldg(&L.atoms[i].w)) & 0xff;
-            e += inter(t, m.cx[i], m.cy[i], m.cz[i], gxs[s], gys[s], gzs[s]);
-        }
+    // 3b: grid term per atom; its gradient seeds the atom's force
+    for (int i = lane; i < L.na; i += 32) {
+        const int t = __float_as_int(__ldg(&L.atoms[i].w)) & 0xff;
+        float gx, gy, gz;
+        const float4 ci = m.c[i];
+        e += inter(t, ci.x, ci.y, ci.z, gx, gy, gz);
+        if (want_grad) { m.fx[i] = gx; m.fy[i] = gy; m.fz[i] = gz; }
     }
-    // 4: intra pairs
-    for (int p = lane; p < L.np; p += 32) {
-        const int2 pr = __ldg(&L.pairs[p]);
-        const int a = pr.x & 0xffff, b = pr.x >> 16;
-        const float rx = m.cx[b] - m.cx[a], ry = m.cy[b] - m.cy[a], rz = m.cz[b] - m.cz[a];
-        const float r2 = rx * rx + ry * ry + rz * rz;
-        float Fx = 0.f, Fy = 0.f, Fz = 0.f;
-        if (r2 < 64.f) {
-            float dor;
-            e += pair_term(smooth, pr.y, r2, v_intra, dor);
-            Fx = dor * rx; Fy = dor * ry; Fz = dor * rz;
+    if (want_grad) __syncwarp();
+    // 4: intra pairs.  Pairs are sorted by their second atom b; each lane
+    // takes a contiguous segment, keeps b's coordinates and force in
+    // registers while b repeats, and adds the force on a with an atomic.
+    {
+        const int p0 = (lane * L.np) >> 5, p1 = ((lane + 1) * L.np) >> 5;
+        int cur_b = -1;
+        float4 cb = make_float4(0.f, 0.f, 0.f, 0.f);
+        float bx = 0.f, by = 0.f, bz = 0.f;
+        int2 nxt = (p0 < p1) ? __ldg(&L.pairs[p0]) : make_int2(0, 0);
+        for (int p = p0; p < p1; ++p) {
+            const int2 pr = nxt;
+            if (p + 1 < p1) nxt = __ldg(&L.pairs[p + 1]);
+            const int a = pr.x & 0xffff, b = pr.x >> 16;
+            if (b != cur_b) {
+                if (want_grad && cur_b >= 0) {
+                    atomicAdd(&m.fx[cur_b], bx); atomicAdd(&m.fy[cur_b], by); atomicAdd(&m.fz[cur_b], bz);
+                }
+                cur_b = b;
+                cb = m.c[b];
+                bx = by = bz = 0.f;
+            }
+            const float4 ca = m.c[a];
+            const float rx = cb.x - ca.x, ry = cb.y - ca.y, rz = cb.z - ca.z;
+            const float r2 = rx * rx + ry * ry + rz * rz;
+            if (r2 < 64.f) {
+                float dor;
+                e += pair_term(smooth, pr.y, r2, v_intra, dor);
+                if (want_grad) {
+                    const float Fx = dor * rx, Fy = dor * ry, Fz = dor * rz;
+                    atomicAdd(&m.fx[a], -Fx); atomicAdd(&m.fy[a], -Fy); atomicAdd(&m.fz[a], -Fz);
+                    bx += Fx; by += Fy; bz += Fz;
+                }
+            }
         }
-        if (want_grad) { m.px[p] = Fx; m.py[p] = Fy; m.pz[p] = Fz; }
+        if (want_grad && cur_b >= 0) {
+            atomicAdd(&m.fx[cur_b], bx); atomicAdd(&m.fy[cur_b], by); atomicAdd(&m.fz[cur_b], bz);
+        }
     }
     e = warp_sum(e);
     if (!want_grad) return e;
     __syncwarp();
-    // 5: per-atom forces
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const int i = lane + 32 * s;
-        if (i < L.na) {
-            float fx = gxs[s], fy = gys[s], fz = gzs[s];
-            const int b0 = __ldg(&L.csr_off[i]), b1 = __ldg(&L.csr_off[i + 1]);
-            for (int q = b0; q < b1; ++q) {
-                const int ent = __ldg(&L.csr[q]);
-                const int p = ent >> 1;
-                if (ent & 1) { fx += m.px[p]; fy += m.py[p]; fz += m.pz[p]; }
-                else { fx -= m.px[p]; fy -= m.py[p]; fz -= m.pz[p]; }
-            }
-            m.fx[i] = fx; m.fy[i] = fy; m.fz[i] = fz;
-        }
-    }
-    __syncwarp();
-    // 6: own force and moment about the root origin per body
+    // 6: own force and moment about the root origin per body.  Atoms are
+    // grouped by body, so a segmented warp scan sums each body's atoms and
+    // the last lane of each segment adds the result to the body.
     const float ox = m.x[0], oy = m.x[1], oz = m.x[2];
-    for (int k = lane; k < L.nn; k += 32) {
-        const int b0 = __ldg(&L.nodes[k].atom_begin), b1 = __ldg(&L.nodes[k].atom_end);
-        float F0 = 0.f, F1 = 0.f, F2 = 0.f, M0 = 0.f, M1 = 0.f, M2 = 0.f;
-        for (int i = b0; i < b1; ++i) {
+    for (int k = lane; k < 6 * L.nn; k += 32) m.ns[k] = 0.f;
+    __syncwarp();
+    for (int base = 0; base < L.na; base += 32) {
+        const int i = base + lane;
+        int key = -1 - lane;
+        float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (i < L.na) {
+            key = (__float_as_int(__ldg(&L.atoms[i].w)) >> 8) & 0xff;
+            const float4 ci = m.c[i];
             const float fx = m.fx[i], fy = m.fy[i], fz = m.fz[i];
-            const float dx = m.cx[i] - ox, dy = m.cy[i] - oy, dz = m.cz[i] - oz;
-            F0 += fx; F1 += fy; F2 += fz;
-            M0 += dy * fz - dz * fy;
-            M1 += dz * fx - dx * fz;
-            M2 += dx * fy - dy * fx;
+            const float dx = ci.x - ox, dy = ci.y - oy, dz = ci.z - oz;
+            v[0] = fx; v[1] = fy; v[2] = fz;
+            v[3] = dy * fz - dz * fy;
+            v[4] = dz * fx - dx * fz;
+            v[5] = dx * fy - dy * fx;
         }
-        float* ns = m.ns + 6 * k;
-        ns[0] = F0; ns[1] = F1; ns[2] = F2; ns[3] = M0; ns[4] = M1; ns[5] = M2;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int ko = __shfl_up_sync(0xffffffffu, key, off);
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                const float o = __shfl_up_sync(0xffffffffu, v[j], off);
+                if (lane >= off && ko == key) v[j] += o;
+            }
+        }
+        const int kn = __shfl_down_sync(0xffffffffu, key, 1);
+        if (i < L.na && (lane == 31 || kn != key)) {
+            float* ns = m.ns + 6 * key;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) atomicAdd(&ns[j], v[j]);
+        }
     }
     __syncwarp();
     // 7: subtree sums, torques and the pose gradient
@@ -343,16 +363,15 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             m.g[0] = F0; m.g[1] = F1; m.g[2] = F2; m.g[3] = M0; m.g[4] = M1; m.g[5] = M2;
         } else {
             const float* nd = m.nd + kNodeF * k;
-            const float dx = nd[4] - ox, dy = nd[5] - oy, dz = nd[6] - oz;
+            const float dx = nd[3] - ox, dy = nd[7] - oy, dz = nd[11] - oz;
             const float T0 = M0 - (dy * F2 - dz * F1);
             const float T1 = M1 - (dz * F0 - dx * F2);
             const float T2 = M2 - (dx * F1 - dy * F0);
-            const float* R = nd + 7;
             const NodeRec& n = L.nodes[k];
             const float u0 = __ldg(&n.axis[0]), u1 = __ldg(&n.axis[1]), u2 = __ldg(&n.axis[2]);
-            const float a0 = R[0] * u0 + R[3] * u1 + R[6] * u2;
-            const float a1 = R[1] * u0 + R[4] * u1 + R[7] * u2;
-            const float a2 = R[2] * u0 + R[5] * u1 + R[8] * u2;
+            const float a0 = nd[0] * u0 + nd[1] * u1 + nd[2] * u2;
+            const float a1 = nd[4] * u0 + nd[5] * u1 + nd[6] * u2;
+            const float a2 = nd[8] * u0 + nd[9] * u1 + nd[10] * u2;
             m.g[6 + k - 1] = T0 * a0 + T1 * a1 + T2 * a2;
         }
     }

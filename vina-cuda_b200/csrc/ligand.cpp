@@ -1,6 +1,5 @@
 // Ligand ingestion: validates a vd_ligand_desc and packs the device blob
-// (heavy atoms only, rigid bodies in pre-order, intra pairs and the per-atom
-// incidence lists the force gather uses).
+// (heavy atoms only, rigid bodies in pre-order, intra pairs).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -51,6 +50,25 @@ bool preorder_ok(const int32_t* parent, int nn) {
     return true;
 }
 
+// Orders pairs by their second atom b.  The energy kernel gives each lane a
+// contiguous segment of this list and keeps atom b's coordinates and force in
+// registers while b stays the same; inside a row of equal b, the first atoms
+// are rotated by b so lanes entering new rows do not all hit the same atom.
+std::vector<int2> order_pairs(const std::vector<int2>& in) {
+    std::vector<int2> out(in);
+    std::stable_sort(out.begin(), out.end(), [](const int2& x, const int2& y) {
+        return (x.x >> 16) != (y.x >> 16) ? (x.x >> 16) < (y.x >> 16) : (x.x & 0xffff) < (y.x & 0xffff);
+    });
+    for (size_t r0 = 0; r0 < out.size();) {
+        size_t r1 = r0;
+        while (r1 < out.size() && (out[r1].x >> 16) == (out[r0].x >> 16)) ++r1;
+        const size_t len = r1 - r0;
+        std::rotate(out.begin() + r0, out.begin() + r0 + (size_t(out[r0].x >> 16) * 13) % len, out.begin() + r1);
+        r0 = r1;
+    }
+    return out;
+}
+
 }  // namespace
 }  // namespace vd
 
@@ -99,6 +117,7 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     }
     const int P = int(pairs.size());
     VD_CHECK(P <= kMaxPairs, VD_ERR_CAPACITY, "vd_add_ligand: more than 4096 intra pairs");
+    pairs = order_pairs(pairs);
 
     auto xyz = [&](int i, int k) { return d->xyz[3 * size_t(i) + k]; };
     // body geometry (tree.h:230-262): origin, unit axis from the parent-side atom
@@ -155,18 +174,6 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     }
     for (auto& r : nodes)
         if (r.atom_begin > r.atom_end) r.atom_begin = r.atom_end = 0;
-    // incidence lists: entry = pair << 1 | (atom is the pair's second atom)
-    std::vector<std::vector<int>> inc(nh);
-    for (int p = 0; p < P; ++p) {
-        inc[pairs[p].x & 0xffff].push_back(p << 1);
-        inc[pairs[p].x >> 16].push_back((p << 1) | 1);
-    }
-    std::vector<int32_t> csr_off(nh + 1, 0), csr;
-    for (int i = 0; i < nh; ++i) {
-        csr_off[i + 1] = csr_off[i] + int(inc[i].size());
-        csr.insert(csr.end(), inc[i].begin(), inc[i].end());
-    }
-
     HostLigand L;
     LigHeader& H = L.h;
     std::memset(&H, 0, sizeof(H));
@@ -175,23 +182,18 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     H.n_pairs = P;
     H.ntors = nn - 1;
     H.max_depth = max_depth;
-    H.n_csr = int(csr.size());
     auto words = [](size_t bytes) { return int32_t((bytes + 15) / 16); };
     H.off_atoms = 4;
     H.off_nodes = H.off_atoms + nh;
     H.off_pairs = H.off_nodes + 3 * nn;
-    H.off_csr = H.off_pairs + words(size_t(P) * sizeof(int2));
-    H.off_csr_list = H.off_csr + words((nh + 1) * sizeof(int32_t));
-    const int32_t total = H.off_csr_list + words(std::max<size_t>(1, csr.size()) * sizeof(int32_t));
-    H.conf_indep = float(d->num_tors);
+    const int32_t total = H.off_pairs + std::max<int32_t>(1, words(size_t(P) * sizeof(int2)));
+    H.num_tors = float(d->num_tors);
     L.blob.assign(size_t(total), make_float4(0, 0, 0, 0));
     char* base = reinterpret_cast<char*>(L.blob.data());
     std::memcpy(base, &H, sizeof(H));
     std::memcpy(base + 16 * size_t(H.off_atoms), atoms.data(), atoms.size() * sizeof(float4));
     std::memcpy(base + 16 * size_t(H.off_nodes), nodes.data(), nodes.size() * sizeof(NodeRec));
     if (P) std::memcpy(base + 16 * size_t(H.off_pairs), pairs.data(), pairs.size() * sizeof(int2));
-    std::memcpy(base + 16 * size_t(H.off_csr), csr_off.data(), csr_off.size() * sizeof(int32_t));
-    if (!csr.empty()) std::memcpy(base + 16 * size_t(H.off_csr_list), csr.data(), csr.size() * sizeof(int32_t));
     L.heavy_index = heavy_index;
     L.n_all_atoms = na;
     L.num_tors = d->num_tors;

@@ -56,9 +56,9 @@ __global__ void __launch_bounds__(32 * kPoseWarps) pose_kernel(PoseParams p) {
             kinematics(L, s.m, lane);
             float* dst = p.xyz_out + size_t(pose) * 3 * L.na;
             for (int i = lane; i < L.na; i += 32) {
-                dst[3 * i] = s.m.cx[i];
-                dst[3 * i + 1] = s.m.cy[i];
-                dst[3 * i + 2] = s.m.cz[i];
+                dst[3 * i] = s.m.c[i].x;
+                dst[3 * i + 1] = s.m.c[i].y;
+                dst[3 * i + 2] = s.m.c[i].z;
             }
         } else {
             const float e = rilc_bfgs(L, s, p.G, p.smooth, p.ep, p.max_steps, lane, evals);
@@ -128,6 +128,15 @@ vd_status vd_energy_grad_device(vd_ctx* h, int32_t lig, int32_t n, const float* 
     VD_CUDA(cudaSetDevice(c.device));
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
     return run_pose_kernel<1>(c, lig, n, poses, ep, e, g, nullptr, nullptr, 0, s);
+}
+
+vd_status vd_energy_device(vd_ctx* h, int32_t lig, int32_t n, const float* poses, const vd_eval_params* ep,
+                           float* e, void* stream) {
+    VD_CHECK(h && poses && e, VD_ERR_ARG, "vd_energy_device: NULL argument");
+    Ctx& c = h->c;
+    VD_CUDA(cudaSetDevice(c.device));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+    return run_pose_kernel<0>(c, lig, n, poses, ep, e, nullptr, nullptr, nullptr, 0, s);
 }
 
 static vd_status pose_host(vd_ctx* h, int32_t lig, int32_t n, const float* poses, const vd_eval_params* ep,

@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(256) cluster_kernel(ClusterParams p) {
             const float* c = kc + size_t(j) * 3 * L.na;
             float acc = 0.f;
             for (int i = lane; i < L.na; i += 32) {
-                const float dx = m.cx[i] - c[3 * i], dy = m.cy[i] - c[3 * i + 1], dz = m.cz[i] - c[3 * i + 2];
+                const float dx = m.c[i].x - c[3 * i], dy = m.c[i].y - c[3 * i + 1], dz = m.c[i].z - c[3 * i + 2];
                 acc += dx * dx + dy * dy + dz * dz;
             }
             acc = warp_sum(acc);
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) cluster_kernel(ClusterParams p) {
         }
         if (close) continue;
         float* c = kc + size_t(nk) * 3 * L.na;
-        for (int i = lane; i < L.na; i += 32) { c[3 * i] = m.cx[i]; c[3 * i + 1] = m.cy[i]; c[3 * i + 2] = m.cz[i]; }
+        for (int i = lane; i < L.na; i += 32) { c[3 * i] = m.c[i].x; c[3 * i + 1] = m.c[i].y; c[3 * i + 2] = m.c[i].z; }
         if (lane == 0) p.kept[li * VD_MAX_MODES + nk] = item;
         ++nk;
         __syncwarp();
@@ -297,8 +297,8 @@ __global__ void __launch_bounds__(32 * kRefineWarps) refine_kernel(RefineParams 
             kinematics(L, s.m, lane);
             bool ok = true;  // non_cache::within, margin 1e-4
             for (int i = lane; i < L.na; i += 32) {
-                if (m_out(s.m.cx[i], p.R.gb[0], p.R.ge[0]) || m_out(s.m.cy[i], p.R.gb[1], p.R.ge[1]) ||
-                    m_out(s.m.cz[i], p.R.gb[2], p.R.ge[2]))
+                if (m_out(s.m.c[i].x, p.R.gb[0], p.R.ge[0]) || m_out(s.m.c[i].y, p.R.gb[1], p.R.ge[1]) ||
+                    m_out(s.m.c[i].z, p.R.gb[2], p.R.ge[2]))
                     ok = false;
             }
             inside = __all_sync(0xffffffffu, ok);

@@ -48,9 +48,9 @@ __device__ __forceinline__ float norm_angle(float x) {  // common.h:316-340
 __device__ __forceinline__ float4 quat_increment(float4 q, float r0, float r1, float r2) {
     const float ang = sqrtf(r0 * r0 + r1 * r1 + r2 * r2);
     if (ang > FLT_EPSILON) {
-        const float inv = 1.f / ang;
+        const float inv = __fdividef(1.f, ang);
         float s, c;
-        sincosf(0.5f * norm_angle(ang), &s, &c);
+        __sincosf(0.5f * norm_angle(ang), &s, &c);
         q = qmul(make_float4(c, s * r0 * inv, s * r1 * inv, s * r2 * inv), q);
     }
     const float n2 = q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
@@ -230,7 +230,7 @@ __device__ __forceinline__ void mutate_pose(const LigView& L, const WarpMem& m, 
         kinematics(L, m, lane);
         float acc = 0.f;
         for (int i = lane; i < L.na; i += 32) {
-            const float dx = m.cx[i] - m.x[0], dy = m.cy[i] - m.x[1], dz = m.cz[i] - m.x[2];
+            const float dx = m.c[i].x - m.x[0], dy = m.c[i].y - m.x[1], dz = m.c[i].z - m.x[2];
             acc += dx * dx + dy * dy + dz * dz;
         }
         acc = warp_sum(acc);

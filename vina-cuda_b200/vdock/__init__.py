@@ -13,7 +13,7 @@ import os
 import numpy as np
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_PATH = os.path.join(PKG_DIR, "libvdock.so")
+LIB_PATH = os.environ.get("VDOCK_LIB") or os.path.join(PKG_DIR, "libvdock.so")  # VDOCK_LIB: another build
 
 MAX_MODES = 20
 MAX_TORS = 48
@@ -59,7 +59,8 @@ class Stats(C.Structure):
 EXPORTS = [
     "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_scoring", "vd_set_receptor",
     "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
-    "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_pose_coords",
+    "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
+    "vd_pose_coords",
     "vd_local_opt", "vd_mc_chains", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score",
     "vd_get_tables", "vd_pdbqt_ligand", "vd_pdbqt_receptor", "vd_pdbqt_write_model", "vd_pdbqt_free",
     "vd_conf_to_coords",
@@ -88,6 +89,7 @@ def lib():
         L.vd_energy.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.POINTER(EvalParams), _fp]
         L.vd_energy_grad.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.POINTER(EvalParams), _fp, _fp]
         L.vd_energy_grad_device.argtypes = [_vp, C.c_int32, C.c_int32, _vp, C.POINTER(EvalParams), _vp, _vp, _vp]
+        L.vd_energy_device.argtypes = [_vp, C.c_int32, C.c_int32, _vp, C.POINTER(EvalParams), _vp, _vp]
         L.vd_pose_coords.argtypes = [_vp, C.c_int32, C.c_int32, _fp, _fp]
         L.vd_local_opt.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.POINTER(EvalParams), C.c_int32, _fp,
                                    C.POINTER(C.c_int64)]
@@ -100,8 +102,8 @@ def lib():
         for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_scoring", "vd_set_receptor",
                      "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_get_grid", "vd_add_ligand",
                      "vd_ligand_info", "vd_clear_ligands", "vd_energy", "vd_energy_grad",
-                     "vd_energy_grad_device", "vd_pose_coords", "vd_local_opt", "vd_mc_chains",
-                     "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_get_tables"):
+                     "vd_energy_grad_device", "vd_energy_device", "vd_pose_coords", "vd_local_opt",
+                     "vd_mc_chains", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_get_tables"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -253,6 +255,10 @@ class Context:
     def energy_grad_device(self, lig, n, poses_ptr, e_ptr, g_ptr, stream_ptr=0, ep=None):
         _check(self.L.vd_energy_grad_device(self.h, lig, n, _vp(poses_ptr), C.byref(ep or eval_params()),
                                             _vp(e_ptr), _vp(g_ptr), _vp(stream_ptr or None)))
+
+    def energy_device(self, lig, n, poses_ptr, e_ptr, stream_ptr=0, ep=None):
+        _check(self.L.vd_energy_device(self.h, lig, n, _vp(poses_ptr), C.byref(ep or eval_params()), _vp(e_ptr),
+                                       _vp(stream_ptr or None)))
 
     def pose_coords(self, lig, poses):
         p, pp = _f(poses)
