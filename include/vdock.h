@@ -162,6 +162,21 @@ vd_status vd_local_opt(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, float* pose
  * (seed, lig_id, chain), so the batched and plain forms give equal chains. */
 vd_status vd_mc_chains(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,
                        float* poses_out, float* e_out, int64_t* evals);
+/* Same chains as vd_mc_chains (same kernel and random streams) for callers
+ * that cannot allocate device memory when they dock -- code recording into a
+ * CUDA graph, where an allocation breaks the capture, or hosts that reserve
+ * their whole device budget up front.  No counterpart in the reference.
+ * It allocates nothing: parameters, counters and results pass through a
+ * static device array of VD_NOALLOC_SCRATCH_BYTES that every GPU loading the
+ * library holds until exit; calls needing more are rejected
+ * (VD_ERR_CAPACITY).  All calls on a device share that array and it keeps
+ * the last call's contents, so calls whose GPU work overlaps race: serialise
+ * them.  Ligands must already be on the device (one allocating call after
+ * vd_add_ligand).  The first call on a device looks up the array's address
+ * once; make it before any stream capture. */
+#define VD_NOALLOC_SCRATCH_BYTES (4u << 20)
+vd_status vd_mc_chains_noalloc(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,
+                               float* poses_out, float* e_out, int64_t* evals);
 /* Plain drop-in form: one ligand per launch, then clustering, GPU refinement
  * and rescoring (main.cpp:423-489). */
 vd_status vd_dock_plain(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,

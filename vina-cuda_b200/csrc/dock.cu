@@ -9,7 +9,9 @@
 // chains.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <string>
 
 #include "dock.h"
 #include "launch.h"
@@ -283,3 +285,131 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Monte-Carlo chains without any device allocation.
+//
+// Some callers cannot call cudaMalloc at the moment they dock: code that
+// records its GPU work into a CUDA graph (an allocation inside stream capture
+// breaks the capture), and host applications that reserve their whole device
+// memory budget up front and forbid allocations afterwards.  This entry point
+// keeps its launch parameters, counters and per-chain results in one
+// statically sized device array instead of the context's growable scratch.
+//
+// Limits and sharing: the array holds VD_NOALLOC_SCRATCH_BYTES; a call whose
+// chains do not fit is rejected with VD_ERR_CAPACITY.  Every GPU that loads
+// the library holds the array until the process exits.  All calls on a
+// device share it and it keeps the previous call's contents (counters are
+// cleared by each call), so calls whose GPU work overlaps race with each
+// other: serialise them.  The first call on a device looks up the array's
+// device address with that device current (one-time set-up); make that first
+// call before any stream capture.
+namespace {
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[VD_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+vd_status noalloc_address(int device, char** out) {
+    VD_CHECK(device >= 0 && device < 64, VD_ERR_ARG, "vd_mc_chains_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        VD_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));  // the device is current here
+        g_noalloc_addr[device] = p;
+    }
+    *out = static_cast<char*>(g_noalloc_addr[device]);
+    return VD_OK;
+}
+
+}  // namespace
+
+extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_search_params* sp, float* poses_out,
+                                          float* e_out, int64_t* evals) {
+    VD_CHECK(h && sp && poses_out && e_out, VD_ERR_ARG, "vd_mc_chains_noalloc: NULL argument");
+    Ctx& c = h->c;
+    VD_CHECK(lig >= 0 && lig < int(c.ligs.size()), VD_ERR_ARG, "vd_mc_chains_noalloc: bad ligand id");
+    VD_CHECK(sp->n_chains > 0, VD_ERR_ARG, "vd_mc_chains_noalloc: n_chains must be positive");
+    VD_CHECK(c.has_box, VD_ERR_ARG, "vd_mc_chains_noalloc: no box set");
+    VD_CHECK(!c.pool_dirty && c.d_pool, VD_ERR_ARG,
+             "vd_mc_chains_noalloc: ligands not on the device yet; make one allocating call "
+             "(e.g. vd_mc_chains or vd_energy) after vd_add_ligand");
+    VD_CUDA(cudaSetDevice(c.device));
+    char* base = nullptr;
+    vd_status st = noalloc_address(c.device, &base);
+    if (st != VD_OK) return st;
+    DockParams p{};
+    st = make_map_view(c, p.G);
+    if (st != VD_OK) return st;
+    st = check_ligand_maps(c, lig);
+    if (st != VD_OK) return st;
+    const HostLigand& L = c.ligs[lig];
+    int depth = 0, steps = 0;
+    search_defaults(L, *sp, depth, steps);
+    const int n = sp->n_chains, nc = 7 + L.h.ntors;
+    // layout: [0,256) counters | [256,512) launch parameters | [512,..) results
+    const size_t conf_bytes = ((size_t(n) * nc * sizeof(float)) + 255) & ~size_t(255);
+    const size_t need = 512 + conf_bytes + size_t(n) * sizeof(float);
+    VD_CHECK(need <= VD_NOALLOC_SCRATCH_BYTES, VD_ERR_CAPACITY,
+             "vd_mc_chains_noalloc: " + std::to_string(n) + " chains of " + std::to_string(nc) +
+                 " floats exceed the static scratch of VD_NOALLOC_SCRATCH_BYTES");
+    unsigned long long* d_cnt = reinterpret_cast<unsigned long long*>(base);
+    char* prm = base + 256;
+    int64_t* d_off = reinterpret_cast<int64_t*>(prm);
+    int32_t* d_pre = reinterpret_cast<int32_t*>(prm + 16);
+    uint32_t* d_uid = reinterpret_cast<uint32_t*>(prm + 32);
+    int32_t* d_depth = reinterpret_cast<int32_t*>(prm + 48);
+    int32_t* d_steps = reinterpret_cast<int32_t*>(prm + 64);
+    float* d_conf = reinterpret_cast<float*>(base + 512);
+    float* d_e = reinterpret_cast<float*>(base + 512 + conf_bytes);
+    struct {
+        int64_t off;
+        int64_t pad0;
+        int32_t pre[4];
+        uint32_t uid[4];
+        int32_t depth[4];
+        int32_t steps[4];
+    } hp = {L.pool_offset, 0, {0, n, 0, 0}, {uint32_t(lig), 0, 0, 0}, {depth, 0, 0, 0}, {steps, 0, 0, 0}};
+    VD_CUDA(cudaMemsetAsync(d_cnt, 0, 256, c.stream));  // counters start at zero on every call
+    VD_CUDA(cudaMemcpyAsync(prm, &hp, sizeof(hp), cudaMemcpyHostToDevice, c.stream));
+    p.pool = c.d_pool;
+    p.lig_off = d_off;
+    p.prefix = d_pre;
+    p.lig_uid = d_uid;
+    p.depth = d_depth;
+    p.bfgs_steps = d_steps;
+    p.n_ligs = 1;
+    p.total_items = n;
+    p.smooth = c.d_smooth;
+    p.ep = {float(sp->hunt_cap[0]), float(sp->hunt_cap[1]), 1e6f};
+    p.seed = sp->seed;
+    p.temperature = float(sp->temperature > 0 ? sp->temperature : 1.2);
+    p.amplitude = float(sp->amplitude > 0 ? sp->amplitude : 2.0);
+    for (int d = 0; d < 3; ++d) {
+        p.lo[d] = float(c.geom.begin[d]);
+        p.hi[d] = float(c.geom.end[d]);
+    }
+    p.out_conf = d_conf;
+    p.stride = nc;
+    p.out_e = d_e;
+    p.queue = nullptr;  // one warp per chain: no work queue
+    p.evals = d_cnt;
+    p.lig_evals = d_cnt + 1;
+    p.warp_floats = lig_warp_floats(L) + 4 * pad4(nc);
+    const int wpb = 4;
+    const size_t smem = size_t(p.warp_floats) * wpb * sizeof(float);
+    VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "vd_mc_chains_noalloc: ligand too large for the kernel");
+    p.warps_per_block = wpb;
+    auto k = dock_kernel<false>;
+    VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    k<<<(n + wpb - 1) / wpb, 32 * wpb, smem, c.stream>>>(p);
+    VD_CUDA(cudaGetLastError());
+    VD_CUDA(cudaMemcpyAsync(poses_out, d_conf, size_t(n) * nc * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    VD_CUDA(cudaMemcpyAsync(e_out, d_e, size_t(n) * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    unsigned long long ev = 0;
+    VD_CUDA(cudaMemcpyAsync(&ev, d_cnt, sizeof(ev), cudaMemcpyDeviceToHost, c.stream));
+    VD_CUDA(cudaStreamSynchronize(c.stream));
+    if (evals) *evals = int64_t(ev);
+    return VD_OK;
+}

@@ -61,7 +61,7 @@ EXPORTS = [
     "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
     "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
     "vd_pose_coords",
-    "vd_local_opt", "vd_mc_chains", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score",
+    "vd_local_opt", "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score",
     "vd_get_tables", "vd_pdbqt_ligand", "vd_pdbqt_receptor", "vd_pdbqt_write_model", "vd_pdbqt_free",
     "vd_conf_to_coords",
 ]
@@ -94,6 +94,7 @@ def lib():
         L.vd_local_opt.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.POINTER(EvalParams), C.c_int32, _fp,
                                    C.POINTER(C.c_int64)]
         L.vd_mc_chains.argtypes = [_vp, C.c_int32, C.POINTER(SearchParams), _fp, _fp, C.POINTER(C.c_int64)]
+        L.vd_mc_chains_noalloc.argtypes = [_vp, C.c_int32, C.POINTER(SearchParams), _fp, _fp, C.POINTER(C.c_int64)]
         L.vd_dock_plain.argtypes = [_vp, C.c_int32, C.POINTER(SearchParams), C.POINTER(DockResult)]
         L.vd_dock_batched.argtypes = [_vp, _ip, C.c_int32, C.POINTER(SearchParams), C.POINTER(DockResult)]
         L.vd_refine.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.c_int32, _fp]
@@ -103,7 +104,7 @@ def lib():
                      "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_get_grid", "vd_add_ligand",
                      "vd_ligand_info", "vd_clear_ligands", "vd_energy", "vd_energy_grad",
                      "vd_energy_grad_device", "vd_energy_device", "vd_pose_coords", "vd_local_opt",
-                     "vd_mc_chains", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_get_tables"):
+                     "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_get_tables"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -281,6 +282,15 @@ class Context:
         e, epp = _f(np.zeros(n, dtype=np.float32))
         ev = C.c_int64()
         _check(self.L.vd_mc_chains(self.h, lig, C.byref(sp), pp, epp, C.byref(ev)))
+        return p, e, ev.value
+
+    def mc_chains_noalloc(self, lig, sp):
+        """vd_mc_chains through the entry point that allocates no device memory."""
+        n = sp.n_chains
+        p, pp = _f(np.zeros((n, 7 + self.ntors[lig]), dtype=np.float32))
+        e, epp = _f(np.zeros(n, dtype=np.float32))
+        ev = C.c_int64()
+        _check(self.L.vd_mc_chains_noalloc(self.h, lig, C.byref(sp), pp, epp, C.byref(ev)))
         return p, e, ev.value
 
     @staticmethod
