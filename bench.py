@@ -118,6 +118,12 @@ def lig_bytes(lig):
     return 32 * heavy + 16 * len(lig["pairs"])
 
 
+# DRAM bytes per evaluation of dock_kernel from one ncu capture of this
+# workload (profiles/dock_kernel_wide_box_screen.txt): 12.07 GB over 15.9 M
+# evaluations; the bench scales it by the evaluations of each launch.
+DOCK_DRAM_BYTES_PER_EVAL = 758.0
+
+
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -285,8 +291,10 @@ def run_ours(a):
                        "gbs": grid_bytes / (min(grid_ms) / 1e3) / 1e9,
                        "frac_of_hbm": grid_bytes / (min(grid_ms) / 1e3) / 1e9 / hbm},
         "roofline": {"kernel": "dock_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
-                     "peak_source": src, "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
-                     "note": "algorithmic bytes = evals x (32 x heavy atoms + 16 x intra pairs)"},
+                     "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": DOCK_DRAM_BYTES_PER_EVAL * evals / K,
+                     "note": "algorithmic bytes = evals x (32 x heavy atoms + 16 x intra pairs); traffic = "
+                             "ncu DRAM bytes per evaluation x evaluations per launch"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk,
