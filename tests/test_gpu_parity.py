@@ -70,9 +70,9 @@ def test_grid_all_17_types_and_odd_box(vd):
         assert err.max() <= GRID_TOL, (t, err.max())
 
 
-def make_ligand_ctx(vd, n_atoms=40, n_tors=10, box=24.0, seed=3):
+def make_ligand_ctx(vd, n_atoms=40, n_tors=10, box=24.0, seed=3, radius=30.0):
     from vdock import synth
-    ctx, orc, _, _ = setup_pair(vd, rec_atoms=2000, radius=30.0, box=box)
+    ctx, orc, _, _ = setup_pair(vd, rec_atoms=2000, radius=radius, box=box)
     lig = synth.ligand(n_atoms, n_tors, seed)
     types = sorted(set(int(t) for t in lig["xs"]))
     ctx.build_grids(types)
@@ -189,3 +189,72 @@ def test_plain_and_batched_forms_compute_identical_chains(vd):
     r_batch = ctx.dock_batched([lc], sp)[0]
     np.testing.assert_array_equal(r_plain["energy"], r_batch["energy"])
     np.testing.assert_array_equal(r_plain["pose"], r_batch["pose"])
+
+
+def test_score_matches_oracle_eval_adjusted(vd):
+    """vd_score (FP64 rescoring on the direct-sum score) equals the oracle's
+    eval_adjusted (model.cpp:1428-1431) and eval_intramolecular
+    (model.cpp:1375-1420) to 1e-3 kcal/mol on the same poses."""
+    from vdock import synth
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=30, n_tors=6, seed=23, box=24.0)
+    poses = synth.random_poses(20, ctx.ntors[lc], -2.0, 2.0, seed=6)
+    adj, intra = ctx.score(lc, poses)
+    i0 = orc.intramolecular(lo, poses[0].astype(np.float64))
+    for i, p in enumerate(poses):
+        pd = p.astype(np.float64)
+        assert abs(intra[i] - orc.intramolecular(lo, pd)) <= E_TOL
+        ref = orc.eval_adjusted(lo, pd, i0)
+        assert abs(adj[i] - ref) <= E_TOL + 1e-6 * abs(ref), (i, adj[i], ref)
+
+
+def test_refine_matches_oracle_distribution(vd):
+    """vd_refine (refine_structure, main.cpp:139-157: dense BFGS on the
+    direct-sum score, slope ramp) against the oracle on the same starts: each
+    returned energy is its pose's direct-sum energy, and the refined energies
+    agree as distributions (paired median within 0.1 kcal/mol)."""
+    from vdock import synth
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=26, n_tors=5, seed=29, box=24.0)
+    # start from locally optimised poses, as refinement does in the pipeline
+    starts = synth.random_poses(40, ctx.ntors[lc], -1.5, 1.5, seed=8)
+    _, starts, _ = ctx.local_opt(lc, starts, 20)
+    e_gpu, p_gpu = ctx.refine(lc, starts, 15)
+    e_ref = []
+    for i, s in enumerate(starts):
+        e, _, _ = orc.refine(lo, s.astype(np.float64), 15)
+        e_ref.append(e)
+        if e_gpu[i] < 1e30:
+            g, _ = orc.eval_deriv(lo, p_gpu[i].astype(np.float64), v=(1000, 1000, 1000), slope=1e6, noncache=True)
+            # the last ramp stage's slope may differ from 1e6 only when atoms leave the box
+            assert abs(g - e_gpu[i]) <= 2e-3 * max(1.0, abs(g)), (i, g, e_gpu[i])
+    e_ref = np.array(e_ref)
+    ok = (e_gpu < 1e30) & (e_ref < 1e30)
+    assert ok.sum() >= 30
+    assert abs(np.median(e_gpu[ok] - e_ref[ok])) <= 0.1
+
+
+def test_docking_pipeline_matches_oracle_pipeline(vd):
+    """Plain docking (chains -> cluster -> refine -> rescore) against the
+    oracle's restatement of the same pipeline on the same seeds: best final
+    score within 0.3 kcal/mol and the modes sorted, >= 1 A apart, within the
+    energy range.  Receptor and box of the plain docking configuration
+    (2,000 atoms in a 40 A ball, 20 A box)."""
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=20, n_tors=4, seed=31, box=20.0, radius=40.0)
+    sp = vd.search_params(seed=5, n_chains=512, search_depth=6, max_bfgs_steps=15, num_modes=9, energy_range=3.0)
+    r = ctx.dock_plain(lc, sp)
+    e = r["energy"]
+    assert 1 <= len(e) <= 9 and np.all(np.diff(e) >= -1e-6) and e[-1] - e[0] <= 3.0 + 1e-6
+    assert np.all(r["rmsd_ub"][1:] >= 1.0 - 1e-4) and r["rmsd_lb"][0] == 0.0
+    conf, ec, _ = orc.mc_chains(lo, 5, lc, 6, 15, 0, 512, threads=8)
+    kept = orc.cluster(lo, conf, ec, 1.0, 20)
+    refined = []
+    for i in kept:
+        er, c, _ = orc.refine(lo, conf[i], 15)
+        if er < 1e30:
+            refined.append((er, c))
+    refined.sort(key=lambda t: t[0])
+    ib = orc.intramolecular(lo, refined[0][1])
+    best_ref = min(orc.eval_adjusted(lo, c, ib) for _, c in refined)
+    assert e[0] < 0 and abs(e[0] - best_ref) <= 0.3, (e[0], best_ref)
+    # the returned score of mode 1 is the score of the returned pose
+    p0 = r["pose"][0].astype(np.float64)
+    assert abs(orc.eval_adjusted(lo, p0, orc.intramolecular(lo, p0)) - e[0]) <= 2e-3

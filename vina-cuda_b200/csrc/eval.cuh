@@ -6,10 +6,10 @@
 //        q_k = q_root * aa_j1 * ... * aa_k,  o_k = o_root + R_root * w_k
 //      (rotation about a body-fixed axis; equals tree.h:282-292)
 //   3. lanes = atoms: coordinates, trilinear grid term (grid.cpp:50-160)
-//   4. lanes = segments of the pair list sorted by second atom: intra pair
-//      term; the force on the second atom is accumulated in registers and
-//      the force on the first atom is added with a shared-memory atomic
-//      (model.cpp:1241-1256)
+//   4. lanes = segments of the pair list sorted by second atom, two pairs
+//      per iteration: intra pair term; the force on the second atom is
+//      accumulated in registers, the force on the first atom is added with a
+//      shared-memory atomic (model.cpp:1241-1256)
 //   6. lanes = bodies: own force and moment about the root origin
 //   7. lanes = bodies: subtree sums over the pre-order range [k, end_k),
 //        torque T_k = M_k - (o_k - o_root) x F_k, dE/dtorsion = T_k . axis_k
@@ -188,23 +188,27 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
     __syncwarp();
 }
 
-// grid.cpp:50-160 in FP32: trilinear value, gradient, curl, out-of-box penalty.
+// grid.cpp:50-160 in FP32: trilinear value, gradient, curl, out-of-box
+// penalty.  Outside the box a coordinate is clamped to the nearest cell
+// (fraction 0 below, 1 above), the gradient component is replaced by
+// slope * region and the penalty adds slope * distance outside.
 __device__ __forceinline__ float grid_term(const MapView& G, const float* map, float px, float py, float pz,
                                            float v, float slope, float& gx, float& gy, float& gz) {
-    float s[3] = {(px - G.init[0]) * G.factor[0], (py - G.init[1]) * G.factor[1], (pz - G.init[2]) * G.factor[2]};
-    float miss[3] = {0.f, 0.f, 0.f};
-    int region[3], a[3];
+    const float pc[3] = {px, py, pz};
+    float fr[3], miss = 0.f, reg[3];
+    int a[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        if (s[d] < 0.f) {
-            miss[d] = -s[d]; region[d] = -1; a[d] = 0; s[d] = 0.f;
-        } else if (s[d] >= G.dmo[d]) {
-            miss[d] = s[d] - G.dmo[d]; region[d] = 1; a[d] = G.n[d] - 2; s[d] = 1.f;
-        } else {
-            region[d] = 0; a[d] = int(s[d]); s[d] -= float(a[d]);
-        }
+        const float s = (pc[d] - G.init[d]) * G.factor[d];
+        const float lo = fmaxf(-s, 0.f), hi = fmaxf(s - G.dmo[d], 0.f);
+        miss += (lo + hi) * G.finv[d];
+        reg[d] = (s < 0.f) ? -1.f : ((s >= G.dmo[d]) ? 1.f : 0.f);
+        const float sc = fminf(fmaxf(s, 0.f), G.dmo[d]);
+        const int ai = min(int(sc), G.n[d] - 2);
+        a[d] = ai;
+        fr[d] = (s >= G.dmo[d]) ? 1.f : sc - float(ai);
     }
-    const float penalty = slope * (miss[0] * G.finv[0] + miss[1] * G.finv[1] + miss[2] * G.finv[2]);
+    const float penalty = slope * miss;
     const size_t row = size_t(G.pitch);
     const size_t plane = row * size_t(G.n[1]);
     const float* b = map + size_t(a[2]) * plane + size_t(a[1]) * row + a[0];
@@ -212,22 +216,19 @@ __device__ __forceinline__ float grid_term(const MapView& G, const float* map, f
     const float f010 = __ldg(b + row), f110 = __ldg(b + row + 1);
     const float f001 = __ldg(b + plane), f101 = __ldg(b + plane + 1);
     const float f011 = __ldg(b + plane + row), f111 = __ldg(b + plane + row + 1);
-    const float x = s[0], y = s[1], z = s[2];
+    const float x = fr[0], y = fr[1], z = fr[2];
     const float mx = 1.f - x, my = 1.f - y, mz = 1.f - z;
     float f = f000 * mx * my * mz + f100 * x * my * mz + f010 * mx * y * mz + f110 * x * y * mz +
               f001 * mx * my * z + f101 * x * my * z + f011 * mx * y * z + f111 * x * y * z;
     float xg = (f100 - f000) * my * mz + (f110 - f010) * y * mz + (f101 - f001) * my * z + (f111 - f011) * y * z;
     float yg = (f010 - f000) * mx * mz + (f110 - f100) * x * mz + (f011 - f001) * mx * z + (f111 - f101) * x * z;
     float zg = (f001 - f000) * mx * my + (f101 - f100) * x * my + (f011 - f010) * mx * y + (f111 - f110) * x * y;
-    if (f > 0.f) {  // curl (curl.h:31-40)
-        const float t = __fdividef(v, v + f);
-        f *= t;
-        const float t2 = t * t;
-        xg *= t2; yg *= t2; zg *= t2;
-    }
-    gx = G.factor[0] * (region[0] == 0 ? xg : 0.f) + slope * float(region[0]);
-    gy = G.factor[1] * (region[1] == 0 ? yg : 0.f) + slope * float(region[1]);
-    gz = G.factor[2] * (region[2] == 0 ? zg : 0.f) + slope * float(region[2]);
+    const float t = (f > 0.f) ? __fdividef(v, v + f) : 1.f;  // curl (curl.h:31-40)
+    f *= t;
+    const float t2 = t * t;
+    gx = (reg[0] == 0.f) ? G.factor[0] * xg * t2 : slope * reg[0];
+    gy = (reg[1] == 0.f) ? G.factor[1] * yg * t2 : slope * reg[1];
+    gz = (reg[2] == 0.f) ? G.factor[2] * zg * t2 : slope * reg[2];
     return f + penalty;
 }
 
@@ -274,42 +275,63 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     }
     if (want_grad) __syncwarp();
     // 4: intra pairs.  Pairs are sorted by their second atom b; each lane
-    // takes a contiguous segment, keeps b's coordinates and force in
-    // registers while b repeats, and adds the force on a with an atomic.
+    // takes a contiguous segment, two pairs at a time (two table gathers in
+    // flight), keeps b's force in registers while b repeats, and adds the
+    // force on a with an atomic.  Table indices are clamped and pairs past
+    // the cutoff masked, so the loads need no branch.
     {
         const int p0 = (lane * L.np) >> 5, p1 = ((lane + 1) * L.np) >> 5;
         int cur_b = -1;
-        float4 cb = make_float4(0.f, 0.f, 0.f, 0.f);
         float bx = 0.f, by = 0.f, bz = 0.f;
-        int2 nxt = (p0 < p1) ? __ldg(&L.pairs[p0]) : make_int2(0, 0);
-        for (int p = p0; p < p1; ++p) {
-            const int2 pr = nxt;
-            if (p + 1 < p1) nxt = __ldg(&L.pairs[p + 1]);
-            const int a = pr.x & 0xffff, b = pr.x >> 16;
-            if (b != cur_b) {
-                if (want_grad && cur_b >= 0) {
-                    atomicAdd(&m.fx[cur_b], bx); atomicAdd(&m.fy[cur_b], by); atomicAdd(&m.fz[cur_b], bz);
-                }
-                cur_b = b;
-                cb = m.c[b];
-                bx = by = bz = 0.f;
+        auto flush = [&](int nb) {
+            if (want_grad && cur_b >= 0) {
+                atomicAdd(&m.fx[cur_b], bx); atomicAdd(&m.fy[cur_b], by); atomicAdd(&m.fz[cur_b], bz);
             }
-            const float4 ca = m.c[a];
-            const float rx = cb.x - ca.x, ry = cb.y - ca.y, rz = cb.z - ca.z;
-            const float r2 = rx * rx + ry * ry + rz * rz;
-            if (r2 < 64.f) {
-                float dor;
-                e += pair_term(smooth, pr.y, r2, v_intra, dor);
-                if (want_grad) {
-                    const float Fx = dor * rx, Fy = dor * ry, Fz = dor * rz;
-                    atomicAdd(&m.fx[a], -Fx); atomicAdd(&m.fy[a], -Fy); atomicAdd(&m.fz[a], -Fz);
+            cur_b = nb;
+            bx = by = bz = 0.f;
+        };
+        for (int p = p0; p < p1; p += 2) {
+            const bool two = p + 1 < p1;
+            const int2 q0 = __ldg(&L.pairs[p]);
+            const int2 q1 = two ? __ldg(&L.pairs[p + 1]) : q0;
+            const int a0 = q0.x & 0xffff, b0 = q0.x >> 16, a1 = q1.x & 0xffff, b1 = q1.x >> 16;
+            const float4 ca0 = m.c[a0], cb0 = m.c[b0], ca1 = m.c[a1], cb1 = m.c[b1];
+            const float r0x = cb0.x - ca0.x, r0y = cb0.y - ca0.y, r0z = cb0.z - ca0.z;
+            const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
+            const float d0 = r0x * r0x + r0y * r0y + r0z * r0z, d1 = r1x * r1x + r1y * r1y + r1z * r1z;
+            const float rf0 = fminf(32.f * d0, 2047.5f), rf1 = fminf(32.f * d1, 2047.5f);
+            const int i0 = int(rf0), i1 = int(rf1);
+            const float4 t0 = __ldg(smooth + size_t(q0.y) * kBins + i0);
+            const float4 t1 = __ldg(smooth + size_t(q1.y) * kBins + i1);
+            const float w0 = rf0 - float(i0), w1 = rf1 - float(i1);
+            float e0 = t0.x + w0 * (t0.z - t0.x), g0 = t0.y + w0 * (t0.w - t0.y);
+            float e1 = t1.x + w1 * (t1.z - t1.x), g1 = t1.y + w1 * (t1.w - t1.y);
+            const float c0 = (e0 > 0.f) ? __fdividef(v_intra, v_intra + e0) : 1.f;
+            const float c1 = (e1 > 0.f) ? __fdividef(v_intra, v_intra + e1) : 1.f;
+            const bool in0 = d0 < 64.f, in1 = two && d1 < 64.f;
+            e0 = in0 ? e0 * c0 : 0.f;
+            e1 = in1 ? e1 * c1 : 0.f;
+            g0 = in0 ? g0 * c0 * c0 : 0.f;
+            g1 = in1 ? g1 * c1 * c1 : 0.f;
+            e += e0 + e1;
+            if (want_grad) {
+                if (b0 != cur_b) flush(b0);
+                if (in0) {
+                    const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
+                    atomicAdd(&m.fx[a0], -Fx); atomicAdd(&m.fy[a0], -Fy); atomicAdd(&m.fz[a0], -Fz);
                     bx += Fx; by += Fy; bz += Fz;
                 }
+                if (two) {
+                    if (b1 != cur_b) flush(b1);
+                    if (in1) {
+                        const float Fx = g1 * r1x, Fy = g1 * r1y, Fz = g1 * r1z;
+                        atomicAdd(&m.fx[a1], -Fx); atomicAdd(&m.fy[a1], -Fy); atomicAdd(&m.fz[a1], -Fz);
+                        bx += Fx; by += Fy; bz += Fz;
+                    }
+                }
             }
         }
-        if (want_grad && cur_b >= 0) {
-            atomicAdd(&m.fx[cur_b], bx); atomicAdd(&m.fy[cur_b], by); atomicAdd(&m.fz[cur_b], bz);
-        }
+        flush(-1);
     }
     e = warp_sum(e);
     if (!want_grad) return e;
