@@ -10,9 +10,14 @@
 //
 // Launch: one CTA per tile of 16(x) x 8(y) x 8(z) points, 256 threads, each
 // thread owning 4 consecutive x points so every map store is one 128-bit
-// store.  The CTA stages, in shared memory, the receptor atoms whose brick
-// distance to the tile is below the cutoff, taken from a 4 A cell list in
-// deterministic (cell, index) order.
+// store; one launch per group of up to 8 maps.  The CTA stages, in shared
+// memory, the receptor atoms whose brick distance to the tile is below the
+// cutoff, taken from per-type 4 A cell lists in deterministic (receptor type,
+// cell, index) order.  The bin index floor(32 r^2) comes from a rounded-down
+// FP64 add of 2^52 (no FP64->int conversion), every point then reads one
+// 32-byte table row (a zero row beyond the cutoff, so the four loads of a
+// thread issue together) and the accumulators are packed FP32 pairs added
+// with add.rn.f32x2.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -23,8 +28,9 @@ namespace vd {
 namespace {
 
 constexpr int kTileX = 16, kTileY = 8, kTileZ = 8, kThreads = 256;
-constexpr int kStageCap = 1280;   // atoms staged per chunk (40 KB)
+constexpr int kStageCap = 1024;   // atoms staged per chunk (32 KB)
 constexpr double kCellSize = 4.0;
+constexpr int kLutRows = kBins + 1;  // table rows per receptor type; the last is zero
 
 struct StagedAtom {
     double x, y, z;
@@ -38,12 +44,12 @@ struct GridParams {
     int32_t pitch;
     size_t map_stride;
     float* maps;                  // first map of this type group
-    const float* lut;             // [17][kBins][ntp]
-    int32_t ntp;                  // lut row width (multiple of 8)
-    int32_t col0;                 // first lut column of this group
+    const float* lut;             // this group's [receptor types present][kLutRows][NTG]
     int32_t n_out;                // maps written by this group (<= NTG)
-    const StagedAtom* atoms;      // relevant receptor atoms sorted by cell
-    const int32_t* cell_start;    // [cells+1]
+    const StagedAtom* atoms;      // relevant receptor atoms sorted by (type, cell)
+    const int32_t* cell_start;    // [n_rtypes][cells+1] per receptor type
+    int32_t n_rtypes;             // receptor types present
+    int32_t n_cells;
     double cell_org[3];
     int32_t cell_dim[3];
 };
@@ -52,14 +58,78 @@ __device__ __forceinline__ double probe_coord(double init, double finv, int i) {
     return __dadd_rn(init, __dmul_rn(finv, double(i)));
 }
 
-template <int NTG>
-__global__ void __launch_bounds__(kThreads) grid_build_kernel(GridParams p) {
-    __shared__ StagedAtom s_atoms[kStageCap];
-    __shared__ int32_t s_row_count[64];
-    __shared__ int32_t s_row_off[65];
-    __shared__ int32_t s_row_begin[64], s_row_end[64];
+constexpr int kMaxRows = 36;            // (cell rows in y) x (cell rows in z) per tile
+constexpr int kMaxCombos = kTypes * kMaxRows;
+#ifndef VD_GRID_MIN_BLOCKS
+#define VD_GRID_MIN_BLOCKS 2
+#endif
 
-    const int t = threadIdx.x;
+// Block-wide exclusive scan of cnt[0..n) into off[0..n]; n <= kMaxCombos.
+__device__ __forceinline__ void block_scan(const int32_t* cnt, int32_t* off, int32_t* s_warp, int n) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int per = (n + kThreads - 1) / kThreads;
+    const int j0 = min(n, t * per), j1 = min(n, j0 + per);
+    int sum = 0;
+    for (int j = j0; j < j1; ++j) sum += cnt[j];
+    int incl = sum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    int run = incl - sum;
+    for (int w = 0; w < warp; ++w) run += s_warp[w];
+    for (int j = j0; j < j1; ++j) {
+        off[j] = run;
+        run += cnt[j];
+    }
+    if (t == kThreads - 1) off[n] = run;
+    __syncthreads();
+}
+
+// floor(32 * r2) for 0 <= r2 <= 64 on the FP64 pipe: 32 * r2 is exact, and
+// adding 2^52 rounded toward -inf leaves the floor in the low mantissa word.
+__device__ __forceinline__ int bin_of(double r2) {
+    return __double2loint(__fma_rd(r2, 32.0, 4503599627370496.0));
+}
+
+// Two FP32 accumulators in one 64-bit register, added with one packed
+// instruction (each lane rounds exactly like a scalar FP32 add).
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+
+// acc[0..NTG/2) += table row v (NTG floats, 32- or 16-byte aligned).
+template <int NTG>
+__device__ __forceinline__ void add_row(unsigned long long (&acc)[NTG / 2], const float* v) {
+    if constexpr (NTG == 8) {
+        unsigned long long a0, a1, a2, a3;
+        asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];" : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3) : "l"(v));
+        acc[0] = add2(acc[0], a0);
+        acc[1] = add2(acc[1], a1);
+        acc[2] = add2(acc[2], a2);
+        acc[3] = add2(acc[3], a3);
+    } else {
+        unsigned long long a0, a1;
+        asm("ld.global.nc.v2.b64 {%0,%1}, [%2];" : "=l"(a0), "=l"(a1) : "l"(v));
+        acc[0] = add2(acc[0], a0);
+        acc[1] = add2(acc[1], a1);
+    }
+}
+
+template <int NTG>
+__global__ void __launch_bounds__(kThreads, VD_GRID_MIN_BLOCKS) grid_build_kernel(GridParams p) {
+    __shared__ StagedAtom s_atoms[kStageCap];
+    __shared__ int32_t s_cnt[kMaxCombos];
+    __shared__ int32_t s_b[kMaxCombos];
+    __shared__ int32_t s_off[kMaxCombos + 1];
+    __shared__ int32_t s_warp[kThreads / 32];
+    __shared__ int32_t s_keep[kThreads / 32];
+
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int xq = t & 3, ly = (t >> 2) & 7, lz = t >> 5;
     const int x0 = blockIdx.x * kTileX + xq * 4;
     const int y = blockIdx.y * kTileY + ly;
@@ -70,52 +140,33 @@ __global__ void __launch_bounds__(kThreads) grid_build_kernel(GridParams p) {
     const int tx_hi = min(tx_lo + kTileX - 1, p.n[0] - 1);
     const int ty_hi = min(ty_lo + kTileY - 1, p.n[1] - 1);
     const int tz_hi = min(tz_lo + kTileZ - 1, p.n[2] - 1);
-    double lo[3] = {probe_coord(p.init[0], p.finv[0], tx_lo), probe_coord(p.init[1], p.finv[1], ty_lo),
-                    probe_coord(p.init[2], p.finv[2], tz_lo)};
-    double hi[3] = {probe_coord(p.init[0], p.finv[0], tx_hi), probe_coord(p.init[1], p.finv[1], ty_hi),
-                    probe_coord(p.init[2], p.finv[2], tz_hi)};
+    const double lo[3] = {probe_coord(p.init[0], p.finv[0], tx_lo), probe_coord(p.init[1], p.finv[1], ty_lo),
+                          probe_coord(p.init[2], p.finv[2], tz_lo)};
+    const double hi[3] = {probe_coord(p.init[0], p.finv[0], tx_hi), probe_coord(p.init[1], p.finv[1], ty_hi),
+                          probe_coord(p.init[2], p.finv[2], tz_hi)};
     int c_lo[3], c_hi[3];
     for (int d = 0; d < 3; ++d) {
         c_lo[d] = max(0, int(floor((lo[d] - 8.0 - p.cell_org[d]) / kCellSize)));
         c_hi[d] = min(p.cell_dim[d] - 1, int(floor((hi[d] + 8.0 - p.cell_org[d]) / kCellSize)));
     }
     const int ry = max(0, c_hi[1] - c_lo[1] + 1), rz = max(0, c_hi[2] - c_lo[2] + 1);
-    const int n_rows = ry * rz;  // <= 36 for the cell and tile sizes above
-    if (t < n_rows) {
-        const int cy = c_lo[1] + t % ry, cz = c_lo[2] + t / ry;
-        const int base = p.cell_dim[0] * (cy + p.cell_dim[1] * cz);
-        s_row_begin[t] = (c_lo[0] <= c_hi[0]) ? p.cell_start[base + c_lo[0]] : 0;
-        s_row_end[t] = (c_lo[0] <= c_hi[0]) ? p.cell_start[base + c_hi[0] + 1] : 0;
-    }
-    __syncthreads();
+    // rows <= kMaxRows: the host checks the tile span against the cell size
+    const int n_rows = (c_lo[0] <= c_hi[0]) ? min(kMaxRows, ry * rz) : 0;
+    const int n_combo = p.n_rtypes * n_rows;  // (receptor type, row), type-major
 
-    const int warp = t >> 5, lane = t & 31;
-    auto keep = [&](const StagedAtom& a) {
-        double d2 = 0;
-        const double c[3] = {a.x, a.y, a.z};
-        for (int d = 0; d < 3; ++d) {
-            double q = c[d] < lo[d] ? lo[d] - c[d] : (c[d] > hi[d] ? c[d] - hi[d] : 0.0);
-            d2 += q * q;
-        }
-        return d2 < 64.0 + 1e-6;  // conservative: the per-point test below is exact
-    };
-    // Pass 1: per-row counts of atoms near the tile.
-    for (int r = warp; r < n_rows; r += kThreads / 32) {
-        int cnt = 0;
-        for (int i = s_row_begin[r]; i < s_row_end[r]; i += 32) {
-            const bool k = (i + lane < s_row_end[r]) && keep(p.atoms[i + lane]);
-            cnt += __popc(__ballot_sync(0xffffffffu, k));
-        }
-        if (lane == 0) s_row_count[r] = cnt;
+    // Candidate ranges per combo, then their exclusive prefix: candidates are
+    // numbered in (type, cz, cy, cx, index) order.
+    for (int j = t; j < n_combo; j += kThreads) {
+        const int tr = j / n_rows, r = j - tr * n_rows;
+        const int cy = c_lo[1] + r % ry, cz = c_lo[2] + r / ry;
+        const int32_t* cs = p.cell_start + size_t(tr) * (p.n_cells + 1) + p.cell_dim[0] * (cy + p.cell_dim[1] * cz);
+        const int b = __ldg(cs + c_lo[0]), e = __ldg(cs + c_hi[0] + 1);
+        s_b[j] = b;
+        s_cnt[j] = e - b;
     }
     __syncthreads();
-    if (t == 0) {
-        int acc = 0;
-        for (int r = 0; r < n_rows; ++r) { s_row_off[r] = acc; acc += s_row_count[r]; }
-        s_row_off[n_rows] = acc;
-    }
-    __syncthreads();
-    const int total = s_row_off[n_rows];
+    block_scan(s_cnt, s_off, s_warp, n_combo);
+    const int n_cand = s_off[n_combo];
 
     const bool active = (x0 < p.n[0]) && (y < p.n[1]) && (z < p.n[2]);
     double px[4];
@@ -123,57 +174,74 @@ __global__ void __launch_bounds__(kThreads) grid_build_kernel(GridParams p) {
     const double py = probe_coord(p.init[1], p.finv[1], y);
     const double pz = probe_coord(p.init[2], p.finv[2], z);
 
-    float acc[4][NTG];
+    unsigned long long acc[4][NTG / 2];  // maps (2j, 2j+1) of point k
 #pragma unroll
     for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int j = 0; j < NTG; ++j) acc[k][j] = 0.f;
+        for (int j = 0; j < NTG / 2; ++j) acc[k][j] = 0ull;
 
-    for (int chunk = 0; chunk < total; chunk += kStageCap) {
-        // Pass 2: compact the atoms of this chunk into shared memory in order.
-        for (int r = warp; r < n_rows; r += kThreads / 32) {
-            int out = s_row_off[r];
-            for (int i = s_row_begin[r]; i < s_row_end[r]; i += 32) {
-                StagedAtom a;
-                bool k = false;
-                if (i + lane < s_row_end[r]) {
-                    a = p.atoms[i + lane];
-                    k = keep(a);
+    for (int chunk = 0;; chunk += kStageCap) {
+        // Stage the kept candidates with ranks [chunk, chunk + kStageCap),
+        // in candidate order (a block-wide stream compaction).
+        int kept = 0;
+        for (int base = 0; base < n_cand; base += kThreads) {
+            const int i = base + t;
+            bool k = false;
+            StagedAtom a;
+            if (i < n_cand) {
+                int lo_j = 0, hi_j = n_combo;  // last j with s_off[j] <= i
+                while (hi_j - lo_j > 1) {
+                    const int mid = (lo_j + hi_j) >> 1;
+                    if (s_off[mid] <= i) lo_j = mid;
+                    else hi_j = mid;
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, k);
-                const int slot = out + __popc(m & ((1u << lane) - 1u)) - chunk;
-                if (k && slot >= 0 && slot < kStageCap) s_atoms[slot] = a;
-                out += __popc(m);
+                a = p.atoms[s_b[lo_j] + (i - s_off[lo_j])];
+                double d2 = 0;
+                const double c[3] = {a.x, a.y, a.z};
+                for (int d = 0; d < 3; ++d) {
+                    const double q = c[d] < lo[d] ? lo[d] - c[d] : (c[d] > hi[d] ? c[d] - hi[d] : 0.0);
+                    d2 += q * q;
+                }
+                k = d2 < kCutoff2 + 1e-6;  // conservative: the per-point test below is exact
             }
+            const unsigned m = __ballot_sync(0xffffffffu, k);
+            if (lane == 0) s_keep[warp] = __popc(m);
+            __syncthreads();
+            int rank = kept + __popc(m & ((1u << lane) - 1u));
+            int step = 0;
+            for (int w = 0; w < kThreads / 32; ++w) {
+                const int cw = s_keep[w];
+                rank += (w < warp) ? cw : 0;
+                step += cw;
+            }
+            const int slot = rank - chunk;
+            if (k && slot >= 0 && slot < kStageCap) s_atoms[slot] = a;
+            kept += step;
+            __syncthreads();
         }
-        __syncthreads();
-        const int n_here = min(kStageCap, total - chunk);
+        const int n_here = min(kStageCap, kept - chunk);
         if (active) {
             for (int a = 0; a < n_here; ++a) {
                 const StagedAtom at = s_atoms[a];
                 const double dy = __dsub_rn(at.y, py), dz = __dsub_rn(at.z, pz);
                 const double dy2 = __dmul_rn(dy, dy), dz2 = __dmul_rn(dz, dz);
                 if (__dadd_rn(dy2, dz2) > kCutoff2) continue;  // exact: sums are monotone
-                const float* row_base = p.lut + size_t(at.type) * kBins * p.ntp + p.col0;
+                // Every point loads a row; points beyond the cutoff read the
+                // type's zero row (always an L1 hit), so the four loads issue
+                // back to back instead of behind one branch each.
+                const float* row_base = p.lut + at.type * (kLutRows * NTG);
+                int bin[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const double dx = __dsub_rn(at.x, px[k]);
                     const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), dy2), dz2);
-                    if (r2 <= kCutoff2) {
-                        const int bin = __double2int_rz(__dmul_rn(32.0, r2));
-                        const float4* v = reinterpret_cast<const float4*>(row_base + size_t(bin) * p.ntp);
-#pragma unroll
-                        for (int j = 0; j < NTG / 4; ++j) {
-                            const float4 q = __ldg(v + j);
-                            acc[k][4 * j + 0] += q.x;
-                            acc[k][4 * j + 1] += q.y;
-                            acc[k][4 * j + 2] += q.z;
-                            acc[k][4 * j + 3] += q.w;
-                        }
-                    }
+                    bin[k] = r2 <= kCutoff2 ? bin_of(r2) : kBins;
                 }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) add_row<NTG>(acc[k], row_base + bin[k] * NTG);
             }
         }
+        if (kept <= chunk + kStageCap) break;
         __syncthreads();
     }
     if (!active) return;
@@ -181,8 +249,9 @@ __global__ void __launch_bounds__(kThreads) grid_build_kernel(GridParams p) {
 #pragma unroll
     for (int j = 0; j < NTG; ++j) {
         if (j >= p.n_out) break;
-        float4 v = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
-        *reinterpret_cast<float4*>(p.maps + size_t(j) * p.map_stride + off) = v;
+        const int h = j & 1, q = j >> 1;
+        auto f = [&](int k) { return __int_as_float(int(h ? acc[k][q] >> 32 : acc[k][q] & 0xffffffffull)); };
+        *reinterpret_cast<float4*>(p.maps + size_t(j) * p.map_stride + off) = make_float4(f(0), f(1), f(2), f(3));
     }
 }
 
@@ -206,7 +275,6 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
     VD_CUDA(cudaSetDevice(c.device));
     const GridGeom& g = c.geom;
     const int nt = int(needed.size());
-    const int ntp = (nt + 7) & ~7;
 
     // Relevant receptor atoms (szv_grid.cpp:28-42 rule) binned into 4 A cells
     // spanning the box grown by the cutoff.
@@ -234,22 +302,53 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
         rel.push_back({a[0], a[1], a[2], c.rec_xs[i], 0});
         cell_of.push_back(ci[0] + cd[0] * (ci[1] + cd[1] * ci[2]));
     }
+    // per receptor type present: cell list over the same cells, atoms sorted
+    // by (type, cell) so a tile stages them type by type
     const int n_cells = cd[0] * cd[1] * cd[2];
-    std::vector<int32_t> start(n_cells + 1, 0);
-    for (int ce : cell_of) start[ce + 1]++;
-    for (int i = 0; i < n_cells; ++i) start[i + 1] += start[i];
+    std::vector<int> present;
+    for (int tr = 0; tr < kTypes; ++tr)
+        for (const auto& a : rel)
+            if (a.type == tr) { present.push_back(tr); break; }
+    if (present.empty()) present.push_back(0);
+    std::vector<int32_t> start(present.size() * size_t(n_cells + 1), 0);
     std::vector<StagedAtom> sorted(rel.size());
     {
-        std::vector<int32_t> fill(start.begin(), start.end() - 1);
-        for (size_t i = 0; i < rel.size(); ++i) sorted[fill[cell_of[i]]++] = rel[i];
-    }
-    // Table slice [17][kBins][ntp] for the needed ligand types.
-    std::vector<float> lut(size_t(kTypes) * kBins * ntp, 0.f);
-    for (int tr = 0; tr < kTypes; ++tr)
-        for (int j = 0; j < nt; ++j) {
-            const size_t b = size_t(tri_index(tr, needed[j])) * kN;
-            for (int i = 0; i < kBins; ++i) lut[(size_t(tr) * kBins + i) * ntp + j] = float(c.fast[b + i]);
+        size_t base_atom = 0;
+        for (size_t ti = 0; ti < present.size(); ++ti) {
+            int32_t* st = &start[ti * size_t(n_cells + 1)];
+            for (size_t i = 0; i < rel.size(); ++i)
+                if (rel[i].type == present[ti]) st[cell_of[i] + 1]++;
+            st[0] = int32_t(base_atom);
+            for (int i = 0; i < n_cells; ++i) st[i + 1] += st[i];
+            std::vector<int32_t> fill(st, st + n_cells);
+            for (size_t i = 0; i < rel.size(); ++i)
+                if (rel[i].type == present[ti]) sorted[fill[cell_of[i]]++] = rel[i];
+            base_atom = size_t(st[n_cells]);
         }
+    }
+    // remap staged atom types to table rows of the present types
+    std::vector<int> row_of(kTypes, 0);
+    for (size_t ti = 0; ti < present.size(); ++ti) row_of[present[ti]] = int(ti);
+    for (auto& a : sorted) a.type = row_of[a.type];
+    // Table slices per group of up to 8 maps: [receptor types present][kLutRows][w]
+    // with w = 8, or 4 for a last group of at most 4 maps.
+    std::vector<int> grp_w, grp_off;
+    size_t lut_floats = 0;
+    for (int g0 = 0; g0 < nt; g0 += 8) {
+        grp_w.push_back(nt - g0 <= 4 ? 4 : 8);
+        grp_off.push_back(int(lut_floats));
+        lut_floats += present.size() * kLutRows * size_t(grp_w.back());
+    }
+    std::vector<float> lut(lut_floats, 0.f);
+    for (size_t gi = 0; gi < grp_w.size(); ++gi) {
+        const int w = grp_w[gi];
+        for (size_t ti = 0; ti < present.size(); ++ti)
+            for (int j = 0; j < w && 8 * int(gi) + j < nt; ++j) {
+                const size_t b = size_t(tri_index(present[ti], needed[8 * gi + j])) * kN;
+                for (int i = 0; i < kBins; ++i)
+                    lut[grp_off[gi] + (ti * kLutRows + i) * w + j] = float(c.fast[b + i]);
+            }
+    }
 
     const size_t map_stride = size_t(g.pitch) * g.n[1] * g.n[2];
     const size_t bytes_maps = map_stride * nt * sizeof(float);
@@ -280,15 +379,18 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
     }
     p.pitch = g.pitch;
     p.map_stride = map_stride;
-    p.lut = d_lut;
-    p.ntp = ntp;
     p.atoms = d_atoms;
     p.cell_start = d_start;
+    p.n_rtypes = int(present.size());
+    p.n_cells = n_cells;
+    for (int d = 1; d < 3; ++d)  // cell rows a tile can touch in y and z: floor(span / cell) + 2 <= 6
+        VD_CHECK(int(std::floor(((kTileY - 1) * g.finv[d] + 16.0) / kCellSize)) + 2 <= 6, VD_ERR_CAPACITY,
+                 "vd_build_grids: grid spacing too large for the tile");
     dim3 grid((g.n[0] + kTileX - 1) / kTileX, (g.n[1] + kTileY - 1) / kTileY, (g.n[2] + kTileZ - 1) / kTileZ);
     VD_CUDA(cudaEventRecord(c.ev0, c.stream));
     for (int g0 = 0; g0 < nt; g0 += 8) {
         p.maps = c.d_maps + size_t(g0) * map_stride;
-        p.col0 = g0;
+        p.lut = d_lut + grp_off[g0 / 8];
         p.n_out = std::min(8, nt - g0);
         if (nt - g0 <= 4) grid_build_kernel<4><<<grid, kThreads, 0, c.stream>>>(p);
         else grid_build_kernel<8><<<grid, kThreads, 0, c.stream>>>(p);
