@@ -85,7 +85,10 @@ typedef struct {
     double   amplitude;       /* mutation amplitude 2 (monte_carlo.h:71)       */
     double   min_rmsd;        /* cluster radius 1.0                            */
     int32_t  refine;          /* 1 = refine + rescore on the GPU (main.cpp:434)*/
-    int32_t  pad;
+    int32_t  launch_shape;    /* docking kernel shape: 0 = autotuned per
+                                 workload, 1/2/3 = 64/48/40 registers per
+                                 thread (8/10/12 blocks of 4 chains per SM);
+                                 results do not depend on it                */
 } vd_search_params;
 
 typedef struct {
@@ -104,8 +107,11 @@ typedef struct {
     double  grid_ms;             /* last vd_build_grids kernel time             */
     double  dock_ms;             /* last docking kernel time                    */
     double  post_ms;             /* last cluster+refine+rescore kernels time    */
-    int32_t dock_warps_per_block;/* launch shape picked by the autotuner        */
+    int32_t dock_warps_per_block;/* chains per block of the last docking launch  */
     int32_t dock_blocks;
+    int32_t dock_shape;          /* launch_shape of the last docking launch (1-3) */
+    int32_t grid_shape;          /* grid tile of the last build: 1 = 16x8x8 points
+                                    per 256 threads, 2 = 16x8x4 per 128         */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -125,6 +131,10 @@ vd_status vd_grid_dims(vd_ctx* ctx, int32_t npts[3], double begin[3], double end
 /* ---- grid maps: replaces kernel_grid (kernel1.cu:202-249) ----------------- */
 /* Builds one FP32 map per listed XS type over the box; maps stay on device. */
 vd_status vd_build_grids(vd_ctx* ctx, const int32_t* xs_types, int32_t n_types);
+/* Grid tile of later builds: 0 = autotuned (the first build of each box size
+ * times both tiles), 1 = 16x8x8 points per 256 threads, 2 = 16x8x4 per 128.
+ * The maps are bit-identical for every tile. */
+vd_status vd_set_grid_shape(vd_ctx* ctx, int32_t shape);
 /* Copies one map to the host, x fastest: out[x + nx*(y + ny*z)]. */
 vd_status vd_get_grid(vd_ctx* ctx, int32_t xs_type, float* out);
 

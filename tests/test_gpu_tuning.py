@@ -1,0 +1,88 @@
+"""Launch-shape autotuning: every shape the autotuner may pick computes
+bit-identical results, and the autotuner settles on one shape per workload.
+
+* grid maps: the 16x8x8 and 16x8x4 tiles sum each point's receptor atoms in
+  the same global (type, cell, index) order, so the maps are equal bit for bit;
+* Monte-Carlo chains: the 64/48/40-register builds of the docking kernel run
+  the same arithmetic on the same Philox streams, so poses and energies are
+  equal bit for bit, in the plain and the persistent (batched) form.
+"""
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def vd():
+    if not has_gpu():
+        pytest.skip("needs a CUDA device")
+    import vdock
+    return vdock
+
+
+def test_grid_tiles_are_bit_identical_and_tuned(vd):
+    from vdock import synth
+    xyz, xs = synth.receptor(1500, 25.0, 5)
+    ctx = vd.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0.5, -0.25, 0.0], [14.0, 11.0, 9.5])
+    maps = {}
+    for shape in (1, 2):
+        ctx.set_grid_shape(shape)
+        ctx.build_grids(synth.TYPES8 + [11, 12])  # two groups: 8 maps and 2 maps
+        assert ctx.stats()["grid_shape"] == shape
+        maps[shape] = [ctx.grid(t) for t in synth.TYPES8 + [11, 12]]
+    for a, b in zip(maps[1], maps[2]):
+        assert np.array_equal(a, b)
+    ctx.set_grid_shape(0)
+    ctx.build_grids(synth.TYPES8 + [11, 12])  # first autotuned build runs both tiles
+    tuned = ctx.stats()["grid_shape"]
+    ctx.build_grids(synth.TYPES8 + [11, 12])
+    assert ctx.stats()["grid_shape"] in (1, 2)
+    for t, ref in zip(synth.TYPES8 + [11, 12], maps[1]):
+        assert np.array_equal(ctx.grid(t), ref)
+    assert tuned in (1, 2)
+
+
+def _dock_ctx(vd):
+    from vdock import synth
+    xyz, xs = synth.receptor(1200, 30.0, 2)
+    ctx = vd.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0.0, 0.0, 0.0], [16.0] * 3)
+    ctx.build_grids(synth.TYPES8)
+    ligs = [ctx.add_ligand(synth.ligand(na, nt, s)) for na, nt, s in ((18, 3, 1), (27, 6, 2), (36, 9, 3))]
+    return ctx, ligs
+
+
+def test_dock_shapes_are_bit_identical(vd):
+    ctx, ligs = _dock_ctx(vd)
+    ref = None
+    for shape in (1, 2, 3):
+        sp = vd.search_params(seed=11, n_chains=300, search_depth=3, launch_shape=shape)
+        poses, e, ev = ctx.mc_chains(ligs[1], sp)
+        assert ctx.stats()["dock_shape"] == shape
+        if ref is None:
+            ref = (poses, e, ev)
+        else:
+            assert np.array_equal(poses, ref[0]) and np.array_equal(e, ref[1]) and ev == ref[2]
+
+
+def test_batched_shapes_are_bit_identical_and_tuner_settles(vd):
+    ctx, ligs = _dock_ctx(vd)
+    outs = []
+    for shape in (1, 2, 3, 0, 0, 0, 0):
+        sp = vd.search_params(seed=3, n_chains=200, search_depth=2, refine=1, launch_shape=shape)
+        res = ctx.dock_batched(ligs, sp)
+        outs.append((res, ctx.stats()["dock_shape"]))
+    for res, _ in outs[1:]:
+        for a, b in zip(res, outs[0][0]):
+            assert np.array_equal(a["energy"], b["energy"]) and np.array_equal(a["pose"], b["pose"])
+            assert a["bfgs_evals"] == b["bfgs_evals"]
+    # three exploring calls run the three shapes, then the tuned one repeats
+    explored = sorted(s for _, s in outs[3:6])
+    assert explored == [1, 2, 3]
+    assert outs[6][1] in (1, 2, 3)

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/vdock.h"
+#include "tune.h"
 
 namespace vd {
 
@@ -138,6 +139,9 @@ struct Ctx {
     size_t scratch_bytes = 0;
     int32_t* d_counter = nullptr;         // work queue + error words
     vd_stats stats{};
+    // launch-shape autotuners (tune.h); grid_shape_fixed > 0 pins the grid tile
+    Tuner dock_tune, grid_tune;
+    int grid_shape_fixed = 0;
 };
 
 vd_status ensure_scratch(Ctx* c, size_t bytes);

@@ -55,11 +55,10 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
     return lo;
 }
 
-template <bool persistent>
-#ifndef VD_DOCK_MIN_BLOCKS
-#define VD_DOCK_MIN_BLOCKS 8  // 4-warp blocks per SM the register budget targets
-#endif
-__global__ void __launch_bounds__(128, VD_DOCK_MIN_BLOCKS) dock_kernel(DockParams p) {
+// MINB: 4-warp blocks per SM the register budget targets (8/10/12 -> 64/48/40
+// registers per thread); the autotuner picks one per workload.
+template <bool persistent, int MINB>
+__global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* base = reinterpret_cast<float*>(smem4) + size_t(wid) * p.warp_floats;
@@ -128,7 +127,26 @@ __global__ void __launch_bounds__(128, VD_DOCK_MIN_BLOCKS) dock_kernel(DockParam
     if (lane == 0 && evals) atomicAdd(p.evals, (unsigned long long)evals);
 }
 
+using DockFn = void (*)(DockParams);
+template <bool persistent>
+DockFn dock_fn(int shape) {
+    switch (shape) {
+        case 1: return dock_kernel<persistent, 10>;
+        case 2: return dock_kernel<persistent, 12>;
+        default: return dock_kernel<persistent, 8>;
+    }
+}
+
 }  // namespace
+
+int dock_shape_for(Ctx& c, const vd_search_params& sp, uint64_t key) {
+    if (sp.launch_shape >= 1 && sp.launch_shape <= kDockShapes) return sp.launch_shape - 1;
+    return c.dock_tune.pick(key, kDockShapes);
+}
+
+void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals) {
+    if (b.tuned && evals > 0) c.dock_tune.report(b.tune_key, b.shape, ms / double(evals));
+}
 
 // Heuristics of main.cpp:354-391 for RILC-BFGS (atoms = all ligand atoms).
 void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps) {
@@ -144,7 +162,7 @@ void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth
 }
 
 vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
-                      DockBuffers& out, cudaStream_t stream, int warps_per_block_override) {
+                      DockBuffers& out, cudaStream_t stream) {
     VD_CHECK(!ligs.empty(), VD_ERR_ARG, "no ligands");
     VD_CHECK(sp.n_chains > 0, VD_ERR_ARG, "n_chains must be positive");
     VD_CHECK(c.has_box, VD_ERR_ARG, "no box set");
@@ -222,32 +240,30 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
     p.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 2);
     p.lig_evals = out.d_lig_evals;
     p.warp_floats = max_wf;
-    // launch shape: warps per block from the override / autotuner, as many
-    // resident blocks as fit for the persistent form
-    int wpb = warps_per_block_override > 0 ? warps_per_block_override : 4;
-    while (wpb > 1 && size_t(max_wf) * wpb * 4 > 200 * 1024) wpb >>= 1;
+    // launch shape: register budget from the caller or the autotuner, keyed
+    // by form, work items and shared memory per chain
+    const int wpb = 4;
     const size_t smem = size_t(max_wf) * wpb * sizeof(float);
     VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "ligand too large for the docking kernel");
     p.warps_per_block = wpb;
+    out.tune_key = (uint64_t(persistent) << 40) | (uint64_t(ceil_log2(uint64_t(items))) << 32) |
+                   uint64_t(max_wf > 1024);  // above 4 KB per chain, shared memory caps the occupancy
+    out.tuned = sp.launch_shape == 0;
+    out.shape = dock_shape_for(c, sp, out.tune_key);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    VD_CUDA(cudaEventRecord(c.ev0, stream));
+    const DockFn k = persistent ? dock_fn<true>(out.shape) : dock_fn<false>(out.shape);
+    VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int blocks = (items + wpb - 1) / wpb;
     if (persistent) {
-        auto k = dock_kernel<true>;
-        VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
         int per_sm = 0;
         VD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * wpb, smem));
-        per_sm = std::max(1, per_sm);
-        const int blocks = std::min(sms * per_sm, (items + wpb - 1) / wpb);
-        k<<<blocks, 32 * wpb, smem, stream>>>(p);
-        c.stats.dock_blocks = blocks;
-    } else {
-        auto k = dock_kernel<false>;
-        VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-        const int blocks = (items + wpb - 1) / wpb;
-        k<<<blocks, 32 * wpb, smem, stream>>>(p);
-        c.stats.dock_blocks = blocks;
+        blocks = std::min(sms * std::max(1, per_sm), blocks);
     }
+    VD_CUDA(cudaEventRecord(c.ev0, stream));
+    k<<<blocks, 32 * wpb, smem, stream>>>(p);
+    c.stats.dock_blocks = blocks;
+    c.stats.dock_shape = out.shape + 1;
     VD_CUDA(cudaGetLastError());
     VD_CUDA(cudaEventRecord(c.ev1, stream));
     c.stats.dock_warps_per_block = wpb;
@@ -267,7 +283,7 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
     VD_CHECK(lig >= 0 && lig < int(c.ligs.size()), VD_ERR_ARG, "vd_mc_chains: bad ligand id");
     VD_CUDA(cudaSetDevice(c.device));
     DockBuffers b;
-    vd_status st = launch_dock(c, {lig}, *sp, false, b, c.stream, 0);
+    vd_status st = launch_dock(c, {lig}, *sp, false, b, c.stream);
     if (st != VD_OK) return st;
     const int nc = 7 + c.ligs[lig].h.ntors;
     VD_CUDA(cudaMemcpy2DAsync(poses_out, nc * sizeof(float), b.d_conf, b.stride * sizeof(float), nc * sizeof(float),
@@ -280,6 +296,7 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
     VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.dock_ms = ms;
     c.stats.bfgs_evals += int64_t(ev);
+    dock_tune_report(c, b, ms, ev);
     if (evals) *evals = int64_t(ev);
     return VD_OK;
 }
@@ -401,7 +418,7 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     const size_t smem = size_t(p.warp_floats) * wpb * sizeof(float);
     VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "vd_mc_chains_noalloc: ligand too large for the kernel");
     p.warps_per_block = wpb;
-    auto k = dock_kernel<false>;
+    auto k = dock_kernel<false, 8>;
     VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     k<<<(n + wpb - 1) / wpb, 32 * wpb, smem, c.stream>>>(p);
     VD_CUDA(cudaGetLastError());

@@ -16,10 +16,17 @@ struct DockBuffers {
     unsigned long long* d_lig_evals = nullptr;  // [n_ligs] evaluations per ligand
     size_t extra_bytes = 0;         // caller-requested scratch after the outputs
     char* d_extra = nullptr;
+    uint64_t tune_key = 0;          // autotuner key of the launch
+    int shape = 0;                  // launch shape used (0-based)
+    bool tuned = false;             // shape came from the autotuner
 };
+
+constexpr int kDockShapes = 3;      // register budgets 64/48/40 per thread
 
 void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps);
 vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
-                      DockBuffers& out, cudaStream_t stream, int warps_per_block_override);
+                      DockBuffers& out, cudaStream_t stream);
+// Feeds the kernel time per search evaluation of a finished launch to the autotuner.
+void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals);
 
 }  // namespace vd

@@ -278,7 +278,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     // takes a contiguous segment, two pairs at a time (two table gathers in
     // flight), keeps b's force in registers while b repeats, and adds the
     // force on a with an atomic.  Table indices are clamped and pairs past
-    // the cutoff masked, so the loads need no branch.
+    // the cutoff masked (their table loads predicated off).
     {
         const int p0 = (lane * L.np) >> 5, p1 = ((lane + 1) * L.np) >> 5;
         int cur_b = -1;
@@ -301,14 +301,15 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const float d0 = r0x * r0x + r0y * r0y + r0z * r0z, d1 = r1x * r1x + r1y * r1y + r1z * r1z;
             const float rf0 = fminf(32.f * d0, 2047.5f), rf1 = fminf(32.f * d1, 2047.5f);
             const int i0 = int(rf0), i1 = int(rf1);
-            const float4 t0 = __ldg(smooth + size_t(q0.y) * kBins + i0);
-            const float4 t1 = __ldg(smooth + size_t(q1.y) * kBins + i1);
+            const bool in0 = d0 < 64.f, in1 = two && d1 < 64.f;
+            float4 t0 = make_float4(0.f, 0.f, 0.f, 0.f), t1 = t0;
+            if (in0) t0 = __ldg(smooth + size_t(q0.y) * kBins + i0);  // no gather past the cutoff
+            if (in1) t1 = __ldg(smooth + size_t(q1.y) * kBins + i1);
             const float w0 = rf0 - float(i0), w1 = rf1 - float(i1);
             float e0 = t0.x + w0 * (t0.z - t0.x), g0 = t0.y + w0 * (t0.w - t0.y);
             float e1 = t1.x + w1 * (t1.z - t1.x), g1 = t1.y + w1 * (t1.w - t1.y);
             const float c0 = (e0 > 0.f) ? __fdividef(v_intra, v_intra + e0) : 1.f;
             const float c1 = (e1 > 0.f) ? __fdividef(v_intra, v_intra + e1) : 1.f;
-            const bool in0 = d0 < 64.f, in1 = two && d1 < 64.f;
             e0 = in0 ? e0 * c0 : 0.f;
             e1 = in1 ? e1 * c1 : 0.f;
             g0 = in0 ? g0 * c0 * c0 : 0.f;

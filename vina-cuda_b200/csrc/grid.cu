@@ -8,9 +8,9 @@
 // evaluated in double with explicitly rounded operations (no FMA
 // contraction); the table values are FP32 and the sums are FP32.
 //
-// Launch: one CTA per tile of 16(x) x 8(y) x 8(z) points, 256 threads, each
-// thread owning 4 consecutive x points so every map store is one 128-bit
-// store; one launch per group of up to 8 maps.  The CTA stages, in shared
+// Launch: one CTA per tile of 16(x) x 8(y) x TZ(z) points (TZ = 8 or 4,
+// autotuned), 32*TZ threads, each thread owning 4 consecutive x points so
+// every map store is one 128-bit store; one launch per group of up to 8 maps.  The CTA stages, in shared
 // memory, the receptor atoms whose brick distance to the tile is below the
 // cutoff, taken from per-type 4 A cell lists in deterministic (receptor type,
 // cell, index) order.  The bin index floor(32 r^2) comes from a rounded-down
@@ -27,7 +27,7 @@
 namespace vd {
 namespace {
 
-constexpr int kTileX = 16, kTileY = 8, kTileZ = 8, kThreads = 256;
+constexpr int kTileX = 16, kTileY = 8;  // z tile (TZ = 8 or 4) is a launch shape; threads = 32 * TZ
 constexpr int kStageCap = 1024;   // atoms staged per chunk (32 KB)
 constexpr double kCellSize = 4.0;
 constexpr int kLutRows = kBins + 1;  // table rows per receptor type; the last is zero
@@ -60,11 +60,8 @@ __device__ __forceinline__ double probe_coord(double init, double finv, int i) {
 
 constexpr int kMaxRows = 36;            // (cell rows in y) x (cell rows in z) per tile
 constexpr int kMaxCombos = kTypes * kMaxRows;
-#ifndef VD_GRID_MIN_BLOCKS
-#define VD_GRID_MIN_BLOCKS 2
-#endif
-
 // Block-wide exclusive scan of cnt[0..n) into off[0..n]; n <= kMaxCombos.
+template <int kThreads>
 __device__ __forceinline__ void block_scan(const int32_t* cnt, int32_t* off, int32_t* s_warp, int n) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int per = (n + kThreads - 1) / kThreads;
@@ -120,8 +117,11 @@ __device__ __forceinline__ void add_row(unsigned long long (&acc)[NTG / 2], cons
     }
 }
 
-template <int NTG>
-__global__ void __launch_bounds__(kThreads, VD_GRID_MIN_BLOCKS) grid_build_kernel(GridParams p) {
+// TZ = 8: 256 threads, 2 blocks per SM (120 registers); TZ = 4: 128 threads,
+// 4 blocks per SM, twice the blocks for small boxes.
+template <int NTG, int TZ>
+__global__ void __launch_bounds__(32 * TZ, 16 / TZ) grid_build_kernel(GridParams p) {
+    constexpr int kThreads = 32 * TZ, kTileZ = TZ;
     __shared__ StagedAtom s_atoms[kStageCap];
     __shared__ int32_t s_cnt[kMaxCombos];
     __shared__ int32_t s_b[kMaxCombos];
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, VD_GRID_MIN_BLOCKS) grid_build_kerne
         s_cnt[j] = e - b;
     }
     __syncthreads();
-    block_scan(s_cnt, s_off, s_warp, n_combo);
+    block_scan<kThreads>(s_cnt, s_off, s_warp, n_combo);
     const int n_cand = s_off[n_combo];
 
     const bool active = (x0 < p.n[0]) && (y < p.n[1]) && (z < p.n[2]);
@@ -386,25 +386,53 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
     for (int d = 1; d < 3; ++d)  // cell rows a tile can touch in y and z: floor(span / cell) + 2 <= 6
         VD_CHECK(int(std::floor(((kTileY - 1) * g.finv[d] + 16.0) / kCellSize)) + 2 <= 6, VD_ERR_CAPACITY,
                  "vd_build_grids: grid spacing too large for the tile");
-    dim3 grid((g.n[0] + kTileX - 1) / kTileX, (g.n[1] + kTileY - 1) / kTileY, (g.n[2] + kTileZ - 1) / kTileZ);
-    VD_CUDA(cudaEventRecord(c.ev0, c.stream));
-    for (int g0 = 0; g0 < nt; g0 += 8) {
-        p.maps = c.d_maps + size_t(g0) * map_stride;
-        p.lut = d_lut + grp_off[g0 / 8];
-        p.n_out = std::min(8, nt - g0);
-        if (nt - g0 <= 4) grid_build_kernel<4><<<grid, kThreads, 0, c.stream>>>(p);
-        else grid_build_kernel<8><<<grid, kThreads, 0, c.stream>>>(p);
-        VD_CUDA(cudaGetLastError());
+    // Launch shapes (z tile 8 or 4) give bit-identical maps: a point sums its
+    // atoms in global (type, cell, index) order whatever the tile.  The first
+    // build of a box size times both and keeps the faster.
+    const uint64_t key = (uint64_t(ceil_log2(uint64_t(g.n[0]) * g.n[1] * g.n[2])) << 8) | uint64_t((nt + 7) / 8);
+    std::vector<int> shapes;
+    if (c.grid_shape_fixed > 0) shapes.push_back(c.grid_shape_fixed - 1);
+    else if (c.grid_tune.best(key) >= 0) shapes.push_back(c.grid_tune.best(key));
+    else shapes = {0, 1};
+    float best_ms = -1;
+    for (int shape : shapes) {
+        const int tz = shape == 0 ? 8 : 4;
+        dim3 grid((g.n[0] + kTileX - 1) / kTileX, (g.n[1] + kTileY - 1) / kTileY, (g.n[2] + tz - 1) / tz);
+        VD_CUDA(cudaEventRecord(c.ev0, c.stream));
+        for (int g0 = 0; g0 < nt; g0 += 8) {
+            p.maps = c.d_maps + size_t(g0) * map_stride;
+            p.lut = d_lut + grp_off[g0 / 8];
+            p.n_out = std::min(8, nt - g0);
+            const bool narrow = nt - g0 <= 4;
+            if (shape == 0) {
+                if (narrow) grid_build_kernel<4, 8><<<grid, 256, 0, c.stream>>>(p);
+                else grid_build_kernel<8, 8><<<grid, 256, 0, c.stream>>>(p);
+            } else {
+                if (narrow) grid_build_kernel<4, 4><<<grid, 128, 0, c.stream>>>(p);
+                else grid_build_kernel<8, 4><<<grid, 128, 0, c.stream>>>(p);
+            }
+            VD_CUDA(cudaGetLastError());
+        }
+        VD_CUDA(cudaEventRecord(c.ev1, c.stream));
+        VD_CUDA(cudaEventSynchronize(c.ev1));
+        float ms = 0;
+        VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        c.grid_tune.pick(key, 2);
+        c.grid_tune.report(key, shape, ms);
+        if (best_ms < 0 || ms < best_ms) best_ms = ms;
+        c.stats.grid_shape = shape + 1;
     }
-    VD_CUDA(cudaEventRecord(c.ev1, c.stream));
-    VD_CUDA(cudaStreamSynchronize(c.stream));
-    float ms = 0;
-    VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
-    c.stats.grid_ms = ms;
+    c.stats.grid_ms = best_ms;
     c.map_stride = map_stride;
     c.n_maps = nt;
     for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
     for (int j = 0; j < nt; ++j) c.map_slot[needed[j]] = j;
+    return VD_OK;
+}
+
+vd_status vd_set_grid_shape(vd_ctx* h, int32_t shape) {
+    VD_CHECK(h && shape >= 0 && shape <= 2, VD_ERR_ARG, "vd_set_grid_shape: shape must be 0, 1 or 2");
+    h->c.grid_shape_fixed = shape;
     return VD_OK;
 }
 

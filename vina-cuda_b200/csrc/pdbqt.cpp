@@ -181,7 +181,7 @@ std::vector<std::vector<std::pair<int, bool>>> perceive_bonds(const std::vector<
         bool put = false;
         for (auto& b : beads)
             if (d2(A[i].xyz, b.first) < 15.0 * 15.0) { b.second.push_back(i); put = true; break; }
-        if (!put) beads.push_back({A[i].xyz, {i}});
+        if (!put) beads.emplace_back(A[i].xyz, std::vector<int>(1, i));
     }
     std::vector<std::vector<std::pair<int, bool>>> bonds(n);
     for (int i = 0; i < n; ++i) {

@@ -826,7 +826,7 @@ vd_status dock_pipeline(Ctx& c, const std::vector<int>& ligs, const vd_search_pa
     DockBuffers db;
     db.extra_bytes = post_scratch_bytes(int(ligs.size()), 7 + max_nt);
     VD_CUDA(cudaMemsetAsync(c.d_counter, 0, 64, c.stream));
-    vd_status st = launch_dock(c, ligs, sp, persistent, db, c.stream, 0);
+    vd_status st = launch_dock(c, ligs, sp, persistent, db, c.stream);
     if (st != VD_OK) return st;
     float dock_ms = 0;
     VD_CUDA(cudaEventSynchronize(c.ev1));
@@ -843,6 +843,7 @@ vd_status dock_pipeline(Ctx& c, const std::vector<int>& ligs, const vd_search_pa
     c.stats.dock_ms = dock_ms;
     c.stats.post_ms = post_ms;
     c.stats.bfgs_evals += int64_t(ev[0] + ev[1]);
+    dock_tune_report(c, db, dock_ms, ev[0]);
     for (size_t i = 0; i < ligs.size(); ++i) out[i].bfgs_evals = int64_t(lev[i]);  // search evaluations
     return VD_OK;
 }

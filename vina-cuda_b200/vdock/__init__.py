@@ -42,7 +42,7 @@ class SearchParams(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("n_chains", C.c_int32), ("search_depth", C.c_int32),
                 ("max_bfgs_steps", C.c_int32), ("num_modes", C.c_int32), ("energy_range", C.c_double),
                 ("hunt_cap", C.c_double * 3), ("temperature", C.c_double), ("amplitude", C.c_double),
-                ("min_rmsd", C.c_double), ("refine", C.c_int32), ("pad", C.c_int32)]
+                ("min_rmsd", C.c_double), ("refine", C.c_int32), ("launch_shape", C.c_int32)]
 
 
 class DockResult(C.Structure):
@@ -53,12 +53,13 @@ class DockResult(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("bfgs_evals", C.c_int64), ("grid_ms", C.c_double), ("dock_ms", C.c_double),
-                ("post_ms", C.c_double), ("dock_warps_per_block", C.c_int32), ("dock_blocks", C.c_int32)]
+                ("post_ms", C.c_double), ("dock_warps_per_block", C.c_int32), ("dock_blocks", C.c_int32),
+                ("dock_shape", C.c_int32), ("grid_shape", C.c_int32)]
 
 
 EXPORTS = [
     "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_scoring", "vd_set_receptor",
-    "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
+    "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
     "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
     "vd_pose_coords",
     "vd_local_opt", "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score",
@@ -83,6 +84,7 @@ def lib():
         L.vd_grid_dims.argtypes = [_vp, _ip, _dp, _dp]
         L.vd_build_grids.argtypes = [_vp, _ip, C.c_int32]
         L.vd_get_grid.argtypes = [_vp, C.c_int32, _fp]
+        L.vd_set_grid_shape.argtypes = [_vp, C.c_int32]
         L.vd_add_ligand.argtypes = [_vp, C.POINTER(LigandDesc), _ip]
         L.vd_ligand_info.argtypes = [_vp, C.c_int32, _ip, _ip, _ip]
         L.vd_clear_ligands.argtypes = [_vp]
@@ -101,7 +103,7 @@ def lib():
         L.vd_score.argtypes = [_vp, C.c_int32, C.c_int32, _fp, _fp, _fp]
         L.vd_get_tables.argtypes = [_vp, _dp, _dp, _dp]
         for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_scoring", "vd_set_receptor",
-                     "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_get_grid", "vd_add_ligand",
+                     "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand",
                      "vd_ligand_info", "vd_clear_ligands", "vd_energy", "vd_energy_grad",
                      "vd_energy_grad_device", "vd_energy_device", "vd_pose_coords", "vd_local_opt",
                      "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_get_tables"):
@@ -132,13 +134,14 @@ def _f(a):
 
 def search_params(seed=0, n_chains=8192, search_depth=0, max_bfgs_steps=0, num_modes=9,
                   energy_range=3.0, hunt_cap=(10, 10, 10), temperature=1.2, amplitude=2.0,
-                  min_rmsd=1.0, refine=1):
+                  min_rmsd=1.0, refine=1, launch_shape=0):
     s = SearchParams()
     s.seed, s.n_chains, s.search_depth, s.max_bfgs_steps = seed, n_chains, search_depth, max_bfgs_steps
     s.num_modes, s.energy_range = num_modes, energy_range
     for i in range(3):
         s.hunt_cap[i] = hunt_cap[i]
     s.temperature, s.amplitude, s.min_rmsd, s.refine = temperature, amplitude, min_rmsd, refine
+    s.launch_shape = launch_shape
     return s
 
 
@@ -207,6 +210,9 @@ class Context:
     def build_grids(self, types):
         t, tp = _i(types)
         _check(self.L.vd_build_grids(self.h, tp, len(t)))
+
+    def set_grid_shape(self, shape):
+        _check(self.L.vd_set_grid_shape(self.h, shape))
 
     def grid(self, t):
         n, _, _ = self.grid_dims()
