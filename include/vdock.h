@@ -112,6 +112,8 @@ typedef struct {
     int32_t dock_shape;          /* launch_shape of the last docking launch (1-3) */
     int32_t grid_shape;          /* grid tile of the last build: 1 = 16x8x8 points
                                     per 256 threads, 2 = 16x8x4 per 128         */
+    int64_t graph_launches;      /* batched pipelines submitted as a CUDA graph */
+    int64_t graph_instantiations;/* executables built (the rest were updated in place) */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */

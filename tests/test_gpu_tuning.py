@@ -1,5 +1,7 @@
-"""Launch-shape autotuning: every shape the autotuner may pick computes
-bit-identical results, and the autotuner settles on one shape per workload.
+"""Launch-shape autotuning and the graph-captured batched pipeline: every
+shape the autotuner may pick computes bit-identical results, the autotuner
+settles on one shape per workload, and repeated batched calls of one
+topology replay one CUDA graph executable, updated in place.
 
 * grid maps: the 16x8x8 and 16x8x4 tiles sum each point's receptor atoms in
   the same global (type, cell, index) order, so the maps are equal bit for bit;
@@ -86,3 +88,22 @@ def test_batched_shapes_are_bit_identical_and_tuner_settles(vd):
     explored = sorted(s for _, s in outs[3:6])
     assert explored == [1, 2, 3]
     assert outs[6][1] in (1, 2, 3)
+
+
+def test_batched_pipeline_replays_one_graph(vd):
+    ctx, ligs = _dock_ctx(vd)
+    sp = vd.search_params(seed=5, n_chains=128, search_depth=2, refine=1, launch_shape=1)
+    s0 = ctx.stats()
+    ref = ctx.dock_batched(ligs, sp)
+    runs = [ctx.dock_batched(ligs, sp) for _ in range(3)]
+    runs.append(ctx.dock_batched(ligs[::-1], sp)[::-1])  # same topology, other parameters
+    s1 = ctx.stats()
+    assert s1["graph_launches"] - s0["graph_launches"] == 5
+    assert s1["graph_instantiations"] - s0["graph_instantiations"] == 1
+    for res in runs:
+        for a, b in zip(res, ref):
+            assert np.array_equal(a["energy"], b["energy"]) and np.array_equal(a["pose"], b["pose"])
+    plain = [ctx.dock_plain(l, sp) for l in ligs]  # direct launches, no graph
+    assert ctx.stats()["graph_launches"] == s1["graph_launches"]
+    for a, b in zip(plain, ref):
+        assert np.array_equal(a["energy"], b["energy"]) and np.array_equal(a["pose"], b["pose"])

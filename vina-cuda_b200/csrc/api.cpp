@@ -22,6 +22,17 @@ vd_status ensure_scratch(Ctx* c, size_t bytes) {
     return VD_OK;
 }
 
+vd_status ensure_host_stage(Ctx* c, size_t bytes) {
+    if (c->h_stage_bytes >= bytes) return VD_OK;
+    if (c->h_stage) VD_CUDA(cudaFreeHost(c->h_stage));
+    c->h_stage = nullptr;
+    c->h_stage_bytes = 0;
+    const size_t want = bytes + bytes / 4;
+    VD_CUDA(cudaMallocHost(&c->h_stage, want));
+    c->h_stage_bytes = want;
+    return VD_OK;
+}
+
 }  // namespace vd
 
 using namespace vd;
@@ -53,6 +64,7 @@ vd_status vd_create(vd_ctx** out, int device) {
     for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c.ev0) != cudaSuccess || cudaEventCreate(&c.ev1) != cudaSuccess ||
+        cudaEventCreate(&c.ev2) != cudaSuccess ||
         cudaMalloc(&c.d_counter, 64 * sizeof(int32_t)) != cudaSuccess) {
         set_error("vd_create: stream/event/counter allocation failed");
         delete h;
@@ -78,8 +90,11 @@ vd_status vd_destroy(vd_ctx* h) {
     cudaFree(c.d_pool);
     cudaFree(c.d_scratch);
     cudaFree(c.d_counter);
+    if (c.pipe_exec) cudaGraphExecDestroy(c.pipe_exec);
+    if (c.h_stage) cudaFreeHost(c.h_stage);
     if (c.ev0) cudaEventDestroy(c.ev0);
     if (c.ev1) cudaEventDestroy(c.ev1);
+    if (c.ev2) cudaEventDestroy(c.ev2);
     if (c.stream) cudaStreamDestroy(c.stream);
     delete h;
     return VD_OK;

@@ -102,7 +102,7 @@ struct GridGeom {
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
     bool scoring = false;
     double weights[6];
     std::vector<double> fast, se, sd;     // [153][2051] double (host)
@@ -138,13 +138,29 @@ struct Ctx {
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
     int32_t* d_counter = nullptr;         // work queue + error words
+    // batched pipeline: pinned staging of its uploads and results, and the
+    // executable CUDA graph it is recorded into (updated in place per call)
+    void* h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    cudaGraphExec_t pipe_exec = nullptr;
     vd_stats stats{};
     // launch-shape autotuners (tune.h); grid_shape_fixed > 0 pins the grid tile
     Tuner dock_tune, grid_tune;
     int grid_shape_fixed = 0;
 };
 
+// Event record that becomes an event node (usable for timing) when the stream
+// is being captured into a CUDA graph, and a plain record otherwise.
+inline cudaError_t record_event(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    const cudaError_t r = cudaStreamIsCapturing(s, &cs);
+    if (r != cudaSuccess) return r;
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e, s, cudaEventRecordExternal)
+                                               : cudaEventRecord(e, s);
+}
+
 vd_status ensure_scratch(Ctx* c, size_t bytes);
+vd_status ensure_host_stage(Ctx* c, size_t bytes);
 vd_status sync_pool(Ctx* c);
 vd_status ensure_receptor_cells(Ctx* c);
 void build_tables(const double w[6], std::vector<double>& fast, std::vector<double>& se,

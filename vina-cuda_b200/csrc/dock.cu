@@ -161,8 +161,12 @@ void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth
     bfgs_steps = sp.max_bfgs_steps > 0 ? sp.max_bfgs_steps : int(unsigned(30 + L.n_all_atoms) / 3);
 }
 
-vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
-                      DockBuffers& out, cudaStream_t stream) {
+// Host side of a docking launch: checks, heuristics, device scratch layout
+// and the packed parameter arrays; no stream operation (so the enqueue can be
+// recorded into a CUDA graph).  Scratch layout:
+//   [params: off | prefix | uid | depth | steps] [conf] [e] [lig_evals] [extra]
+vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
+                       DockBuffers& out) {
     VD_CHECK(!ligs.empty(), VD_ERR_ARG, "no ligands");
     VD_CHECK(sp.n_chains > 0, VD_ERR_ARG, "n_chains must be positive");
     VD_CHECK(c.has_box, VD_ERR_ARG, "no box set");
@@ -191,31 +195,33 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
     out.items = items;
     out.stride = 7 + max_nt;
     out.prefix = prefix;
-    // device buffers: params arrays + outputs
+    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t b_off = n * sizeof(int64_t), b_pre = (n + 1) * sizeof(int32_t), b_arr = n * sizeof(int32_t);
     const size_t b_conf = size_t(items) * out.stride * sizeof(float), b_e = size_t(items) * sizeof(float);
-    auto al = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t b_lev = n * sizeof(unsigned long long);
-    const size_t total = al(b_off) + al(b_pre) + 3 * al(b_arr) + al(b_conf) + al(b_e) + al(b_lev) + out.extra_bytes;
+    const size_t b_par = al(b_off) + al(b_pre) + 3 * al(b_arr);
+    const size_t total = b_par + al(b_conf) + al(b_e) + al(b_lev) + out.extra_bytes;
     st = ensure_scratch(&c, total);
     if (st != VD_OK) return st;
+    // packed parameter arrays (host) and their device copies at the scratch start
+    out.h_params.assign(b_par, 0);
+    size_t o = 0;
+    auto put = [&](const void* src, size_t bytes) {
+        std::memcpy(out.h_params.data() + o, src, bytes);
+        o += al(bytes);
+    };
     char* s = static_cast<char*>(c.d_scratch);
-    int64_t* d_off = reinterpret_cast<int64_t*>(s); s += al(b_off);
-    int32_t* d_pre = reinterpret_cast<int32_t*>(s); s += al(b_pre);
-    uint32_t* d_uid = reinterpret_cast<uint32_t*>(s); s += al(b_arr);
-    int32_t* d_depth = reinterpret_cast<int32_t*>(s); s += al(b_arr);
-    int32_t* d_steps = reinterpret_cast<int32_t*>(s); s += al(b_arr);
+    out.d_params = s;
+    const int64_t* d_off = reinterpret_cast<const int64_t*>(s + o); put(off.data(), b_off);
+    const int32_t* d_pre = reinterpret_cast<const int32_t*>(s + o); put(prefix.data(), b_pre);
+    const uint32_t* d_uid = reinterpret_cast<const uint32_t*>(s + o); put(uid.data(), b_arr);
+    const int32_t* d_depth = reinterpret_cast<const int32_t*>(s + o); put(depth.data(), b_arr);
+    const int32_t* d_steps = reinterpret_cast<const int32_t*>(s + o); put(steps.data(), b_arr);
+    s += b_par;
     out.d_conf = reinterpret_cast<float*>(s); s += al(b_conf);
     out.d_e = reinterpret_cast<float*>(s); s += al(b_e);
     out.d_lig_evals = reinterpret_cast<unsigned long long*>(s); s += al(b_lev);
     out.d_extra = s;
-    VD_CUDA(cudaMemsetAsync(out.d_lig_evals, 0, b_lev, stream));
-    VD_CUDA(cudaMemcpyAsync(d_off, off.data(), b_off, cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemcpyAsync(d_pre, prefix.data(), b_pre, cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemcpyAsync(d_uid, uid.data(), b_arr, cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemcpyAsync(d_depth, depth.data(), b_arr, cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemcpyAsync(d_steps, steps.data(), b_arr, cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemsetAsync(c.d_counter, 0, 16, stream));
     p.pool = c.d_pool;
     p.lig_off = d_off;
     p.prefix = d_pre;
@@ -260,14 +266,34 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
         VD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 32 * wpb, smem));
         blocks = std::min(sms * std::max(1, per_sm), blocks);
     }
-    VD_CUDA(cudaEventRecord(c.ev0, stream));
-    k<<<blocks, 32 * wpb, smem, stream>>>(p);
+    out.launch = [k, blocks, wpb, smem, p](cudaStream_t stream) {
+        k<<<blocks, 32 * wpb, smem, stream>>>(p);
+        return cudaGetLastError();
+    };
     c.stats.dock_blocks = blocks;
     c.stats.dock_shape = out.shape + 1;
-    VD_CUDA(cudaGetLastError());
-    VD_CUDA(cudaEventRecord(c.ev1, stream));
     c.stats.dock_warps_per_block = wpb;
     return VD_OK;
+}
+
+// Stream side of a docking launch: parameter upload (from params_src, the
+// packed arrays or a pinned copy of them), counter resets, the kernel
+// bracketed by c.ev0 / c.ev1.
+vd_status enqueue_dock(Ctx& c, const DockBuffers& b, const void* params_src, cudaStream_t stream) {
+    VD_CUDA(cudaMemcpyAsync(b.d_params, params_src, b.h_params.size(), cudaMemcpyHostToDevice, stream));
+    VD_CUDA(cudaMemsetAsync(b.d_lig_evals, 0, (b.prefix.size() - 1) * sizeof(unsigned long long), stream));
+    VD_CUDA(cudaMemsetAsync(c.d_counter, 0, 16, stream));
+    VD_CUDA(record_event(c.ev0, stream));
+    VD_CUDA(b.launch(stream));
+    VD_CUDA(record_event(c.ev1, stream));
+    return VD_OK;
+}
+
+vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
+                      DockBuffers& out, cudaStream_t stream) {
+    vd_status st = prepare_dock(c, ligs, sp, persistent, out);
+    if (st != VD_OK) return st;
+    return enqueue_dock(c, out, out.h_params.data(), stream);
 }
 
 }  // namespace vd

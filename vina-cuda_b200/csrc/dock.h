@@ -1,6 +1,7 @@
 // Docking launch interface shared by dock.cu and post.cu.
 #pragma once
 
+#include <functional>
 #include <vector>
 
 #include "common.h"
@@ -19,11 +20,20 @@ struct DockBuffers {
     uint64_t tune_key = 0;          // autotuner key of the launch
     int shape = 0;                  // launch shape used (0-based)
     bool tuned = false;             // shape came from the autotuner
+    std::vector<unsigned char> h_params;  // packed parameter arrays (host)
+    void* d_params = nullptr;             // their device copy
+    std::function<cudaError_t(cudaStream_t)> launch;  // the kernel launch
 };
 
 constexpr int kDockShapes = 3;      // register budgets 64/48/40 per thread
 
 void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps);
+// prepare_dock: host work and device layout (no stream operation);
+// enqueue_dock: upload, counter resets and the kernel between c.ev0 and c.ev1;
+// launch_dock: both.
+vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
+                       DockBuffers& out);
+vd_status enqueue_dock(Ctx& c, const DockBuffers& b, const void* params_src, cudaStream_t stream);
 vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
                       DockBuffers& out, cudaStream_t stream);
 // Feeds the kernel time per search evaluation of a finished launch to the autotuner.

@@ -14,6 +14,8 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <functional>
+#include <string>
 
 #include "dock.h"
 #include "launch.h"
@@ -699,9 +701,20 @@ int refine_warp_floats(const HostLigand& L) {
 
 inline size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// cluster -> gather -> refine -> score for the ligands of one dock launch.
-vd_status post_process(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, DockBuffers& db,
-                       vd_dock_result* out, cudaStream_t stream) {
+// Host side of cluster -> gather -> refine -> score for the ligands of one
+// dock launch: parameters, device layout in the dock's extra scratch
+// (params: off | prefix | steps | pose ligand | n_in, then kept poses and
+// results) and the kernel launches; no stream operation.
+struct PostPlan {
+    std::vector<unsigned char> h_params;
+    void* d_params = nullptr;
+    vd_dock_result* d_out = nullptr;
+    int n = 0;
+    std::function<cudaError_t(cudaStream_t)> launch;
+};
+
+vd_status prepare_post(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, const DockBuffers& db,
+                       PostPlan& pp) {
     vd_status st = ensure_receptor_cells(&c);
     if (st != VD_OK) return st;
     const int n = int(ligs.size());
@@ -721,24 +734,33 @@ vd_status post_process(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     int sort_n = 1;
     while (sort_n < max_chains) sort_n <<= 1;
     VD_CHECK(sort_n <= 16384, VD_ERR_CAPACITY, "more than 16384 chains per ligand");
-    // scratch after the dock outputs
-    char* s = db.d_extra;
-    int64_t* d_off = reinterpret_cast<int64_t*>(s); s += al256(n * sizeof(int64_t));
-    int32_t* d_pre = reinterpret_cast<int32_t*>(s); s += al256((n + 1) * sizeof(int32_t));
-    int32_t* d_kept = reinterpret_cast<int32_t*>(s); s += al256(size_t(n) * VD_MAX_MODES * sizeof(int32_t));
-    int32_t* d_steps = reinterpret_cast<int32_t*>(s); s += al256(n * sizeof(int32_t));
-    int32_t* d_plig = reinterpret_cast<int32_t*>(s); s += al256(size_t(n) * VD_MAX_MODES * sizeof(int32_t));
-    int32_t* d_nin = reinterpret_cast<int32_t*>(s); s += al256(n * sizeof(int32_t));
-    float* d_rp = reinterpret_cast<float*>(s); s += al256(size_t(n) * VD_MAX_MODES * db.stride * sizeof(float));
-    float* d_re = reinterpret_cast<float*>(s); s += al256(size_t(n) * VD_MAX_MODES * sizeof(float));
-    vd_dock_result* d_out = reinterpret_cast<vd_dock_result*>(s); s += al256(n * sizeof(vd_dock_result));
-    VD_CUDA(cudaMemcpyAsync(d_off, off.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemcpyAsync(d_pre, db.prefix.data(), (n + 1) * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaMemcpyAsync(d_steps, steps.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
     std::vector<int32_t> plig(size_t(n) * VD_MAX_MODES), nin(n, VD_MAX_MODES);
     for (int i = 0; i < n * VD_MAX_MODES; ++i) plig[i] = i / VD_MAX_MODES;
-    VD_CUDA(cudaMemcpyAsync(d_plig, plig.data(), plig.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
-    VD_CUDA(cudaEventRecord(c.ev0, stream));
+    // parameter arrays (host), mirrored at the start of the extra scratch
+    size_t o = 0;
+    const size_t b_par = al256(n * sizeof(int64_t)) + al256((n + 1) * sizeof(int32_t)) + al256(n * sizeof(int32_t)) +
+                         al256(plig.size() * sizeof(int32_t)) + al256(n * sizeof(int32_t));
+    pp.h_params.assign(b_par, 0);
+    char* s = db.d_extra;
+    pp.d_params = s;
+    auto put = [&](const void* src, size_t bytes) {
+        std::memcpy(pp.h_params.data() + o, src, bytes);
+        char* d = s + o;
+        o += al256(bytes);
+        return d;
+    };
+    const int64_t* d_off = reinterpret_cast<const int64_t*>(put(off.data(), n * sizeof(int64_t)));
+    const int32_t* d_pre = reinterpret_cast<const int32_t*>(put(db.prefix.data(), (n + 1) * sizeof(int32_t)));
+    const int32_t* d_steps = reinterpret_cast<const int32_t*>(put(steps.data(), n * sizeof(int32_t)));
+    const int32_t* d_plig = reinterpret_cast<const int32_t*>(put(plig.data(), plig.size() * sizeof(int32_t)));
+    const int32_t* d_nin = reinterpret_cast<const int32_t*>(put(nin.data(), n * sizeof(int32_t)));
+    s += b_par;
+    int32_t* d_kept = reinterpret_cast<int32_t*>(s); s += al256(size_t(n) * VD_MAX_MODES * sizeof(int32_t));
+    float* d_rp = reinterpret_cast<float*>(s); s += al256(size_t(n) * VD_MAX_MODES * db.stride * sizeof(float));
+    float* d_re = reinterpret_cast<float*>(s); s += al256(size_t(n) * VD_MAX_MODES * sizeof(float));
+    vd_dock_result* d_out = reinterpret_cast<vd_dock_result*>(s);
+    pp.d_out = d_out;
+    pp.n = n;
     // cluster
     ClusterParams cp{};
     cp.pool = c.d_pool;
@@ -755,15 +777,12 @@ vd_status post_process(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     const size_t smem_c = size_t(sort_n) * 8 + size_t(max_wf) * 4 + size_t(VD_MAX_MODES) * 3 * max_na * 4;
     VD_CHECK(smem_c <= 227 * 1024, VD_ERR_CAPACITY, "cluster kernel shared memory exceeds 227 KB");
     VD_CUDA(cudaFuncSetAttribute(cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_c)));
-    cluster_kernel<<<n, 256, smem_c, stream>>>(cp);
-    VD_CUDA(cudaGetLastError());
-    // gather kept poses (missing slots get e = FLT_MAX)
-    gather_kernel<<<n * VD_MAX_MODES, 64, 0, stream>>>(d_kept, db.d_conf, db.d_e, db.stride, n * VD_MAX_MODES,
-                                                       d_rp, d_re);
-    VD_CUDA(cudaGetLastError());
     // refine
-    if (sp.refine) {
-        RefineParams rp{};
+    const bool refine = sp.refine != 0;
+    RefineParams rp{};
+    size_t smem_r = 0;
+    int blocks_r = 0;
+    if (refine) {
         rp.pool = c.d_pool;
         rp.lig_off = d_off;
         rp.pose_lig = d_plig;
@@ -777,12 +796,10 @@ vd_status post_process(Ctx& c, const std::vector<int>& ligs, const vd_search_par
         rp.warp_floats = max_rwf;
         rp.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 4);
         rp.skip_invalid = 1;
-        const size_t smem_r = size_t(max_rwf) * kRefineWarps * 4;
+        smem_r = size_t(max_rwf) * kRefineWarps * 4;
         VD_CHECK(smem_r <= 227 * 1024, VD_ERR_CAPACITY, "refine kernel shared memory exceeds 227 KB");
         VD_CUDA(cudaFuncSetAttribute(refine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_r)));
-        const int blocks = (n * VD_MAX_MODES + kRefineWarps - 1) / kRefineWarps;
-        refine_kernel<<<blocks, 32 * kRefineWarps, smem_r, stream>>>(rp);
-        VD_CUDA(cudaGetLastError());
+        blocks_r = (n * VD_MAX_MODES + kRefineWarps - 1) / kRefineWarps;
     }
     // score
     ScoreParams sc{};
@@ -790,7 +807,6 @@ vd_status post_process(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     sc.lig_off = d_off;
     sc.poses = d_rp;
     sc.e_ref = d_re;
-    VD_CUDA(cudaMemcpyAsync(d_nin, nin.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
     sc.n_in = d_nin;
     sc.stride = db.stride;
     sc.R = rec_view(c);
@@ -802,12 +818,43 @@ vd_status post_process(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     sc.out = d_out;
     const size_t smem_s = size_t(16 * max_nn + 3 * max_na) * 8 + size_t(VD_MAX_MODES) * 3 * max_na * 4;
     VD_CUDA(cudaFuncSetAttribute(score_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_s)));
-    score_kernel<<<n, 32, smem_s, stream>>>(sc);
-    VD_CUDA(cudaGetLastError());
-    VD_CUDA(cudaEventRecord(c.ev1, stream));
-    VD_CUDA(cudaMemcpyAsync(out, d_out, n * sizeof(vd_dock_result), cudaMemcpyDeviceToHost, stream));
+    const int stride = db.stride;
+    const float* conf = db.d_conf;
+    const float* e = db.d_e;
+    pp.launch = [=](cudaStream_t stream) {
+        cluster_kernel<<<n, 256, smem_c, stream>>>(cp);
+        // gather kept poses (missing slots get e = FLT_MAX)
+        gather_kernel<<<n * VD_MAX_MODES, 64, 0, stream>>>(d_kept, conf, e, stride, n * VD_MAX_MODES, d_rp, d_re);
+        if (refine) refine_kernel<<<blocks_r, 32 * kRefineWarps, smem_r, stream>>>(rp);
+        score_kernel<<<n, 32, smem_s, stream>>>(sc);
+        return cudaGetLastError();
+    };
     return VD_OK;
 }
+
+// Stream side: parameter upload, the kernels (ending at c.ev2), the results
+// to out (host, pinned for graph capture).
+vd_status enqueue_post(Ctx& c, const PostPlan& pp, const void* params_src, vd_dock_result* out,
+                       cudaStream_t stream) {
+    VD_CUDA(cudaMemcpyAsync(pp.d_params, params_src, pp.h_params.size(), cudaMemcpyHostToDevice, stream));
+    VD_CUDA(pp.launch(stream));
+    VD_CUDA(record_event(c.ev2, stream));
+    VD_CUDA(cudaMemcpyAsync(out, pp.d_out, pp.n * sizeof(vd_dock_result), cudaMemcpyDeviceToHost, stream));
+    return VD_OK;
+}
+
+// Ends a stream capture left open by an early return.
+struct CaptureGuard {
+    cudaStream_t s;
+    bool open;
+    ~CaptureGuard() {
+        if (open) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s, &g);
+            if (g) cudaGraphDestroy(g);
+        }
+    }
+};
 
 }  // namespace
 
@@ -817,34 +864,92 @@ size_t post_scratch_bytes(int n_ligs, int stride) {
            al256(size_t(n_ligs) * VD_MAX_MODES * 4) + al256(n_ligs * sizeof(vd_dock_result)) + 1024;
 }
 
+// Docking of a ligand list followed by the post-processing.  The batched
+// (persistent) form records the whole sequence -- parameter uploads from a
+// pinned stage, the docking kernel, cluster / gather / refine / score and
+// the result download -- into one CUDA graph, updated in place when the
+// next call records the same topology, and submits it with one launch; the
+// plain form issues the same operations directly, one ligand per launch.
 vd_status dock_pipeline(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
                         vd_dock_result* out) {
     VD_CUDA(cudaSetDevice(c.device));
     for (int l : ligs) VD_CHECK(l >= 0 && l < int(c.ligs.size()), VD_ERR_ARG, "bad ligand id");
     int max_nt = 0;
     for (int l : ligs) max_nt = std::max(max_nt, c.ligs[l].h.ntors);
+    const int n = int(ligs.size());
     DockBuffers db;
-    db.extra_bytes = post_scratch_bytes(int(ligs.size()), 7 + max_nt);
-    VD_CUDA(cudaMemsetAsync(c.d_counter, 0, 64, c.stream));
-    vd_status st = launch_dock(c, ligs, sp, persistent, db, c.stream);
+    db.extra_bytes = post_scratch_bytes(n, 7 + max_nt);
+    vd_status st = prepare_dock(c, ligs, sp, persistent, db);
     if (st != VD_OK) return st;
-    float dock_ms = 0;
-    VD_CUDA(cudaEventSynchronize(c.ev1));
-    VD_CUDA(cudaEventElapsedTime(&dock_ms, c.ev0, c.ev1));
-    st = post_process(c, ligs, sp, db, out, c.stream);
+    PostPlan pp;
+    st = prepare_post(c, ligs, sp, db, pp);
     if (st != VD_OK) return st;
-    unsigned long long ev[2] = {0, 0};
-    std::vector<unsigned long long> lev(ligs.size());
-    VD_CUDA(cudaMemcpyAsync(ev, c.d_counter + 2, 16, cudaMemcpyDeviceToHost, c.stream));
-    VD_CUDA(cudaMemcpyAsync(lev.data(), db.d_lig_evals, lev.size() * 8, cudaMemcpyDeviceToHost, c.stream));
+    // pinned stage: [dock params | post params | results | counters]
+    const size_t b_dp = al256(db.h_params.size()), b_pp = al256(pp.h_params.size());
+    const size_t b_res = al256(n * sizeof(vd_dock_result)), b_cnt = al256((2 + n) * sizeof(unsigned long long));
+    st = ensure_host_stage(&c, b_dp + b_pp + b_res + b_cnt);
+    if (st != VD_OK) return st;
+    unsigned char* hs = static_cast<unsigned char*>(c.h_stage);
+    std::memcpy(hs, db.h_params.data(), db.h_params.size());
+    std::memcpy(hs + b_dp, pp.h_params.data(), pp.h_params.size());
+    vd_dock_result* h_res = reinterpret_cast<vd_dock_result*>(hs + b_dp + b_pp);
+    unsigned long long* h_cnt = reinterpret_cast<unsigned long long*>(hs + b_dp + b_pp + b_res);
+    auto enqueue_all = [&](cudaStream_t s) -> vd_status {
+        vd_status e = enqueue_dock(c, db, hs, s);
+        if (e != VD_OK) return e;
+        e = enqueue_post(c, pp, hs + b_dp, h_res, s);
+        if (e != VD_OK) return e;
+        VD_CUDA(cudaMemcpyAsync(h_cnt, c.d_counter + 2, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+        VD_CUDA(cudaMemcpyAsync(h_cnt + 2, db.d_lig_evals, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                s));
+        return VD_OK;
+    };
+    if (persistent) {
+        CaptureGuard guard{c.stream, false};
+        VD_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+        guard.open = true;
+        st = enqueue_all(c.stream);
+        if (st != VD_OK) return st;
+        cudaGraph_t graph = nullptr;
+        guard.open = false;
+        VD_CUDA(cudaStreamEndCapture(c.stream, &graph));
+        bool updated = false;
+        if (c.pipe_exec) {
+            cudaGraphExecUpdateResultInfo info{};
+            updated = cudaGraphExecUpdate(c.pipe_exec, graph, &info) == cudaSuccess;
+            if (!updated) {
+                cudaGetLastError();  // clear the update failure; a new executable replaces it
+                cudaGraphExecDestroy(c.pipe_exec);
+                c.pipe_exec = nullptr;
+            }
+        }
+        cudaError_t e = cudaSuccess;
+        if (!updated) {
+            e = cudaGraphInstantiate(&c.pipe_exec, graph, 0);
+            ++c.stats.graph_instantiations;
+        }
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            c.pipe_exec = nullptr;
+            set_error(std::string("CUDA graph instantiation failed: ") + cudaGetErrorString(e));
+            return VD_ERR_CUDA;
+        }
+        VD_CUDA(cudaGraphLaunch(c.pipe_exec, c.stream));
+        ++c.stats.graph_launches;
+    } else {
+        st = enqueue_all(c.stream);
+        if (st != VD_OK) return st;
+    }
     VD_CUDA(cudaStreamSynchronize(c.stream));
-    float post_ms = 0;
-    VD_CUDA(cudaEventElapsedTime(&post_ms, c.ev0, c.ev1));
+    float dock_ms = 0, post_ms = 0;
+    VD_CUDA(cudaEventElapsedTime(&dock_ms, c.ev0, c.ev1));
+    VD_CUDA(cudaEventElapsedTime(&post_ms, c.ev1, c.ev2));
+    std::memcpy(out, h_res, n * sizeof(vd_dock_result));
     c.stats.dock_ms = dock_ms;
     c.stats.post_ms = post_ms;
-    c.stats.bfgs_evals += int64_t(ev[0] + ev[1]);
-    dock_tune_report(c, db, dock_ms, ev[0]);
-    for (size_t i = 0; i < ligs.size(); ++i) out[i].bfgs_evals = int64_t(lev[i]);  // search evaluations
+    c.stats.bfgs_evals += int64_t(h_cnt[0] + h_cnt[1]);
+    dock_tune_report(c, db, dock_ms, h_cnt[0]);
+    for (int i = 0; i < n; ++i) out[i].bfgs_evals = int64_t(h_cnt[2 + i]);  // search evaluations
     return VD_OK;
 }
 
