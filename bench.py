@@ -48,6 +48,7 @@ def args_():
     a.add_argument("--e2e-steps", type=int, default=2)
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--cpu-ligands", type=int, default=3, help="whole ligands in the CPU sample")
+    a.add_argument("--no-configs", action="store_true", help="skip the plain / adjoint / uneven-batch lines")
     return a.parse_args()
 
 
@@ -165,6 +166,159 @@ def cpu_baseline(xyz, xs, ligs, chains_per_lig, n_sample):
             "sample": f"{len(desc)} whole ligands (atoms/torsions {', '.join(desc)}), {chains_per_lig} chains "
                       f"each, heuristic depth, top-20 refinement; {total_evals} BFGS evals in {total_t:.1f} s",
             "grid_build_s": t_grid, "bfgs_evals_per_s": total_evals / total_t}
+
+
+def secondary_configs(hbm, cpu):
+    """The reference's other named workloads, measured once each on one GPU
+    (synthetic inputs of the named shapes; seeded):
+      plain_single_ligand : 24-atom / 5-torsion ligand, 2,000-atom receptor,
+                            20 A box, 1,024 chains x 1,000 MC steps, one
+                            vd_dock_plain call (timed after the autotuner's
+                            three exploring calls);
+      adjoint_poses       : 65,536 random poses of a 40-atom / 10-torsion
+                            ligand, energy + gradient (vd_energy_grad_device)
+                            and energy only, inputs resident on the device;
+      batched_uneven      : 512 ligands of 10-60 atoms / 0-15 torsions, 4,000-
+                            atom receptor, 30 A box, 8,192 chains (16 per
+                            ligand) x 2,000 MC steps in one batched call.
+    Each carries the oracle port timed on a bounded sample on the host cores."""
+    import numpy as np
+    import torch
+    import vdock
+    from vdock import synth
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle_lib
+    threads = os.cpu_count() or 1
+    out = {}
+
+    def lig_cost_bytes(lig):
+        return 32 * int((lig["xs"] >= 0).sum()) + 16 * len(lig["pairs"])
+
+    # -- plain single ligand (1,024 chains x 1,000 steps)
+    cfg = synth.CONFIGS["plain"]
+    xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED + 1)
+    lig = synth.ligand(cfg["lig_atoms"], cfg["lig_tors"], SEED + 2)
+    ctx = vdock.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0, 0, 0], [cfg["box"]] * 3)
+    ctx.build_grids(sorted(set(int(t) for t in lig["xs"] if t >= 0)))
+    lid = ctx.add_ligand(lig)
+    sp = vdock.search_params(seed=SEED, n_chains=cfg["chains"], search_depth=cfg["steps"], refine=1)
+    for _ in range(3):
+        ctx.dock_plain(lid, sp)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = ctx.dock_plain(lid, sp)
+    wall = time.perf_counter() - t0
+    st = ctx.stats()
+    line = {"s_per_ligand": wall, "dock_ms": st["dock_ms"], "post_ms": st["post_ms"],
+            "bfgs_evals": int(r["bfgs_evals"]), "bfgs_evals_per_s": r["bfgs_evals"] / (st["dock_ms"] / 1e3),
+            "best_energy": float(r["energy"][0]), "launch_shape": st["dock_shape"]}
+    line["frac_of_hbm"] = line["bfgs_evals_per_s"] * lig_cost_bytes(lig) / 1e9 / hbm
+    ctx.close()
+    if cpu:
+        orc = oracle_lib.Oracle()
+        orc.set_receptor(xyz, xs)
+        orc.set_box([0, 0, 0], [cfg["box"]] * 3)
+        orc.build_grids(sorted(set(int(t) for t in lig["xs"] if t >= 0)))
+        lo = orc.add_ligand(lig)
+        n_s = 128
+        t0 = time.perf_counter()
+        _, _, ev = orc.mc_chains(lo, SEED, lid, cfg["steps"], (30 + lig["n_atoms"]) // 3, 0, n_s, threads=threads)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"s_per_ligand": dt * cfg["chains"] / n_s, "bfgs_evals_per_s": ev / dt,
+                                "cores": threads, "kind": "port",
+                                "sample": f"{n_s} of {cfg['chains']} chains x {cfg['steps']} steps, "
+                                          f"extrapolated to all chains (MC search only)"}
+    out["plain_single_ligand"] = line
+
+    # -- adjoint: 65,536 poses, energy + gradient and energy only
+    cfg = synth.CONFIGS["adjoint"]
+    xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED + 1)
+    lig = synth.ligand(cfg["lig_atoms"], cfg["lig_tors"], SEED + 3)
+    ctx = vdock.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0, 0, 0], [cfg["box"]] * 3)
+    ctx.build_grids(sorted(set(int(t) for t in lig["xs"] if t >= 0)))
+    lid = ctx.add_ligand(lig)
+    n = cfg["poses"]
+    half = cfg["pos_box"] / 2
+    poses = synth.random_poses(n, ctx.ntors[lid], -half, half, SEED + 4)
+    dp = torch.from_numpy(poses).cuda()
+    de = torch.empty(n, device="cuda")
+    dg = torch.empty(n, 6 + ctx.ntors[lid], device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    line = {"poses": n, "pairs": len(lig["pairs"]), "heavy_atoms": int((lig["xs"] >= 0).sum())}
+    for name, call in (("energy_grad", lambda: ctx.energy_grad_device(lid, n, dp.data_ptr(), de.data_ptr(),
+                                                                      dg.data_ptr(), stream)),
+                       ("energy", lambda: ctx.energy_device(lid, n, dp.data_ptr(), de.data_ptr(), stream))):
+        for _ in range(3):
+            call()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            call()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        line[name] = {"ms": ms, "evals_per_s": n / (ms / 1e3),
+                      "gbs": n * lig_cost_bytes(lig) / (ms / 1e3) / 1e9,
+                      "frac_of_hbm": n * lig_cost_bytes(lig) / (ms / 1e3) / 1e9 / hbm}
+    ctx.close()
+    if cpu:
+        orc = oracle_lib.Oracle()
+        orc.set_receptor(xyz, xs)
+        orc.set_box([0, 0, 0], [cfg["box"]] * 3)
+        orc.build_grids(sorted(set(int(t) for t in lig["xs"] if t >= 0)))
+        lo = orc.add_ligand(lig)
+        n_s = 4096
+        t0 = time.perf_counter()
+        for p in poses[:n_s].astype(np.float64):
+            orc.eval_deriv(lo, p)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"evals_per_s": n_s / dt, "cores": 1, "kind": "port",
+                                "sample": f"{n_s} of {n} poses, energy + gradient, one thread"}
+    out["adjoint_poses"] = line
+
+    # -- batched uneven: 512 ligands, 8,192 chains x 2,000 steps
+    cfg = synth.CONFIGS["batched"]
+    xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED + 5)
+    ligs = synth.ligand_set(cfg["ligands"], cfg["atoms"], cfg["tors"], SEED + 6)
+    ctx = vdock.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0, 0, 0], [cfg["box"]] * 3)
+    ctx.build_grids(synth.TYPES8)
+    ids = [ctx.add_ligand(l) for l in ligs]
+    per = cfg["total_chains"] // cfg["ligands"]
+    sp = vdock.search_params(seed=SEED, n_chains=per, search_depth=cfg["steps"], refine=1, launch_shape=1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = ctx.dock_batched(ids, sp)
+    wall = time.perf_counter() - t0
+    st = ctx.stats()
+    evals = sum(int(r["bfgs_evals"]) for r in res)
+    line = {"s": wall, "ligands_per_s": len(ids) / wall, "dock_ms": st["dock_ms"], "post_ms": st["post_ms"],
+            "bfgs_evals": evals, "bfgs_evals_per_s": evals / (st["dock_ms"] / 1e3), "chains_per_ligand": per,
+            "launch_shape": st["dock_shape"], "graph_launches": st["graph_launches"]}
+    ctx.close()
+    if cpu:
+        orc = oracle_lib.Oracle()
+        orc.set_receptor(xyz, xs)
+        orc.set_box([0, 0, 0], [cfg["box"]] * 3)
+        orc.build_grids(synth.TYPES8)
+        t0, cev = time.perf_counter(), 0
+        n_s = 2
+        for i in range(n_s):
+            lo = orc.add_ligand(ligs[i])
+            _, _, ev = orc.mc_chains(lo, SEED, ids[i], cfg["steps"], (30 + ligs[i]["n_atoms"]) // 3, 0, per,
+                                     threads=threads)
+            cev += ev
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"bfgs_evals_per_s": cev / dt, "cores": threads, "kind": "port",
+                                "sample": f"{n_s} of {len(ids)} ligands, {per} chains x {cfg['steps']} steps "
+                                          f"(MC search only)"}
+    out["batched_uneven"] = line
+    return out
 
 
 def run_reference(a):
@@ -305,8 +459,10 @@ def run_ours(a):
         cb = cpu_baseline(xyz, xs, ligs, a.chains, a.cpu_ligands)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         line["grid_build"]["cpu_s"] = cb["grid_build_s"]
-    print(json.dumps(line), flush=True)
     ctx.close()
+    if world == 1 and not a.no_configs:
+        line["configs"] = secondary_configs(hbm, not a.no_cpu_baseline)
+    print(json.dumps(line), flush=True)
 
 
 def main():

@@ -151,8 +151,11 @@ vd_status vd_energy(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* p
                     const vd_eval_params* p, float* e_out);
 vd_status vd_energy_grad(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
                          const vd_eval_params* p, float* e_out, float* g_out);
-/* Same on device buffers already resident (stream = cudaStream_t or NULL for
- * the context stream); asynchronous. */
+/* Same on device buffers already resident, asynchronous on `stream` (a
+ * cudaStream_t; NULL is the CUDA default stream, as for a kernel launch), so
+ * a caller orders it with its own work by passing its stream (e.g. torch's
+ * current stream).  Ligand and map uploads made by earlier calls have
+ * completed before these return. */
 vd_status vd_energy_grad_device(vd_ctx* ctx, int32_t lig_id, int32_t n_poses,
                                 const float* poses_device, const vd_eval_params* p,
                                 float* e_device, float* g_device, void* stream);

@@ -45,6 +45,8 @@ def lib():
         L.or_get_grid.argtypes = [vp, C.c_int, dp]
         L.or_add_ligand.argtypes = [vp, vp]
         L.or_ligand_ntors.argtypes = [vp, C.c_int]
+        L.or_maps_ready.restype = C.c_int
+        L.or_maps_ready.argtypes = [vp, C.c_int]
         L.or_eval_deriv.restype = C.c_double
         L.or_eval_deriv.argtypes = [vp, C.c_int, dp, dp, C.c_double, dp]
         L.or_nc_eval_deriv.restype = C.c_double
@@ -178,7 +180,13 @@ class Oracle:
         self.ntors.append(self.L.or_ligand_ntors(self.h, lig))
         return lig
 
+    def _need_maps(self, lig):
+        if not self.L.or_maps_ready(self.h, lig):
+            raise RuntimeError("oracle: grid maps for the ligand's XS types are not built (build_grids)")
+
     def eval_deriv(self, lig, conf, v=(10, 10, 10), slope=1e6, noncache=False):
+        if not noncache:
+            self._need_maps(lig)
         c, cp = _d(conf)
         vv, vp = _d(v)
         g, gp = _d(np.zeros(6 + self.ntors[lig]))
@@ -214,6 +222,7 @@ class Oracle:
         return self.L.or_rmsd_lower(self.h, lig, ap, bp), self.L.or_rmsd_upper(self.h, lig, ap, bp)
 
     def rilc_bfgs(self, lig, conf, max_steps, v=(10, 10, 10), slope=1e6):
+        self._need_maps(lig)
         c, cp = _d(np.array(conf, dtype=np.float64))
         vv, vp = _d(v)
         ev = C.c_int64(0)
@@ -221,6 +230,8 @@ class Oracle:
         return e, c.copy(), ev.value
 
     def bfgs(self, lig, conf, max_steps, v=(1000, 1000, 1000), slope=1e6, noncache=True):
+        if not noncache:
+            self._need_maps(lig)
         c, cp = _d(np.array(conf, dtype=np.float64))
         vv, vp = _d(v)
         ev = C.c_int64(0)
@@ -234,6 +245,7 @@ class Oracle:
 
     def mc_chains(self, lig, seed, lig_uid, depth, bfgs_steps, chain_begin, chain_end,
                   threads=1, hunt_cap=(10, 10, 10), slope=1e6, temperature=1.2, amplitude=2.0):
+        self._need_maps(lig)
         s = OrSearch()
         s.seed, s.lig_uid, s.search_depth, s.max_bfgs_steps = seed, lig_uid, depth, bfgs_steps
         for i in range(3):

@@ -1047,7 +1047,17 @@ int or_add_ligand(or_ctx* c, const or_ligand* d) {
 }
 int or_ligand_ntors(or_ctx* c, int lig) { return c->ligs[lig].ntors(); }
 
+// 1 when a map exists for every heavy-atom type of the ligand (the cached
+// evaluation reads them); entry points that need the maps return NaN / -1
+// otherwise instead of reading an empty map.
+int or_maps_ready(or_ctx* c, int lig) {
+    for (int t : c->ligs[lig].xs)
+        if (t >= 0 && t < kTypes && c->grids[t].data.empty()) return 0;
+    return 1;
+}
+
 double or_eval_deriv(or_ctx* c, int lig, const double* conf, const double v[3], double slope, double* grad) {
+    if (!or_maps_ready(c, lig)) return std::nan("");
     Frames F;
     std::vector<V3> f;
     return eval_deriv_cache(c, c->ligs[lig], conf, v, slope, grad, F, f);
@@ -1130,6 +1140,7 @@ double or_rmsd_lower(or_ctx* c, int lig, const double* a, const double* b) {
 
 double or_rilc_bfgs(or_ctx* c, int lig, double* conf, const double v[3], double slope, int max_steps,
                     int64_t* evals) {
+    if (!or_maps_ready(c, lig)) return std::nan("");
     const Lig& L = c->ligs[lig];
     Objective obj{c, &L, v, slope, eval_deriv_cache};
     double e = rilc_bfgs(obj, L.ntors(), conf, max_steps);
@@ -1139,6 +1150,7 @@ double or_rilc_bfgs(or_ctx* c, int lig, double* conf, const double v[3], double 
 
 double or_bfgs(or_ctx* c, int lig, double* conf, const double v[3], double slope, int max_steps,
                int use_noncache, int64_t* evals) {
+    if (!use_noncache && !or_maps_ready(c, lig)) return std::nan("");
     const Lig& L = c->ligs[lig];
     Objective obj{c, &L, v, slope, use_noncache ? eval_deriv_noncache : eval_deriv_cache};
     double e = dense_bfgs(obj, L.ntors(), conf, max_steps);
@@ -1152,6 +1164,7 @@ void or_init_conf(or_ctx* c, int lig, uint32_t seed, uint32_t lig_uid, uint32_t 
 
 int64_t or_mc_chains(or_ctx* c, int lig, const or_search* s, int cb, int ce, double* out_conf,
                      double* out_e, int threads) {
+    if (!or_maps_ready(c, lig)) return -1;
     const Lig& L = c->ligs[lig];
     const int nc = 7 + L.ntors();
     std::atomic<int> next(cb);

@@ -51,6 +51,9 @@ int     or_build_grids(or_ctx*, const int32_t* types, int n_types);
 int     or_get_grid(or_ctx*, int xs_type, double* out /* x fastest */);
 int     or_add_ligand(or_ctx*, const or_ligand*);
 int     or_ligand_ntors(or_ctx*, int lig);
+/* 1 when the maps of every heavy-atom type of the ligand are built; the cached
+ * evaluations below return NaN (or_mc_chains: -1) otherwise. */
+int     or_maps_ready(or_ctx*, int lig);
 
 /* conf layout: pos[3], quat[4] (w,x,y,z), torsions[ntors]
  * grad layout: force[3], torque[3], torsion grads[ntors]

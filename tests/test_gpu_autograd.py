@@ -166,3 +166,27 @@ def test_autograd_matches_central_differences(setup):
         assert np.all(err_gpu <= err_ref + tol), (i, (err_gpu - err_ref).max(), tol)
         rigid = np.min(np.abs(fds[:, :6] - g[i][:6]), axis=0)
         assert np.all(rigid <= tol), (i, rigid, tol)
+
+
+def test_device_entry_points_follow_the_callers_stream(setup):
+    """vd_energy_grad_device / vd_energy_device run on the stream they are
+    given: work the caller enqueues after them on that stream sees their
+    results (here a clone on a side stream), equal bit for bit to the
+    host-buffer entry point."""
+    torch, vdock, ctx, orc, lig, lc, lo = setup
+    from vdock import synth
+    nt = ctx.ntors[lc]
+    poses = synth.random_poses(4096, nt, -15.0, 15.0, seed=5)
+    e_ref, g_ref = ctx.energy_grad(lc, poses)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        dp = torch.from_numpy(poses).cuda()
+        de = torch.full((len(poses),), float("nan"), device="cuda")
+        dg = torch.full((len(poses), 6 + nt), float("nan"), device="cuda")
+        de2 = torch.full((len(poses),), float("nan"), device="cuda")
+        ctx.energy_grad_device(lc, len(poses), dp.data_ptr(), de.data_ptr(), dg.data_ptr(), side.cuda_stream)
+        ctx.energy_device(lc, len(poses), dp.data_ptr(), de2.data_ptr(), side.cuda_stream)
+        e_c, g_c, e2_c = de.clone(), dg.clone(), de2.clone()
+    side.synchronize()
+    assert np.array_equal(e_c.cpu().numpy(), e_ref) and np.array_equal(g_c.cpu().numpy(), g_ref)
+    np.testing.assert_allclose(e2_c.cpu().numpy(), e_ref, rtol=0, atol=1e-5 * np.abs(e_ref).max())

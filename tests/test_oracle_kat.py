@@ -161,3 +161,29 @@ def test_philox_known_answer():
     assert O.philox([0xffffffff] * 4, [0xffffffff] * 2) == [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]
     assert O.philox([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344],
                     [0xa4093822, 0x299f31d0]) == [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]
+
+
+def test_oracle_refuses_unbuilt_maps():
+    """The cached evaluations read one map per ligand XS type; with a map
+    missing the oracle raises (and its C entry points return NaN / -1)
+    instead of reading an empty map."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "vina-cuda_b200"))
+    from vdock import synth
+    xyz, xs = synth.receptor(400, 18.0, 3)
+    lig = synth.ligand(18, 3, 4)
+    o = O.Oracle()
+    o.set_receptor(xyz, xs)
+    o.set_box([0.0, 0.0, 0.0], [10.0] * 3)
+    lid = o.add_ligand(lig)
+    conf = np.zeros(7 + o.ntors[lid])
+    conf[3] = 1.0
+    with pytest.raises(RuntimeError):
+        o.eval_deriv(lid, conf)
+    with pytest.raises(RuntimeError):
+        o.mc_chains(lid, 1, 0, 1, 3, 0, 2)
+    assert o.L.or_maps_ready(o.h, lid) == 0
+    o.build_grids(sorted(set(int(t) for t in lig["xs"] if t >= 0)))
+    assert o.L.or_maps_ready(o.h, lid) == 1
+    assert np.isfinite(o.eval_deriv(lid, conf)[0])

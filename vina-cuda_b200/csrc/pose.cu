@@ -126,7 +126,7 @@ vd_status vd_energy_grad_device(vd_ctx* h, int32_t lig, int32_t n, const float* 
     VD_CHECK(h && poses && e && g, VD_ERR_ARG, "vd_energy_grad_device: NULL argument");
     Ctx& c = h->c;
     VD_CUDA(cudaSetDevice(c.device));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
     return run_pose_kernel<1>(c, lig, n, poses, ep, e, g, nullptr, nullptr, 0, s);
 }
 
@@ -135,7 +135,7 @@ vd_status vd_energy_device(vd_ctx* h, int32_t lig, int32_t n, const float* poses
     VD_CHECK(h && poses && e, VD_ERR_ARG, "vd_energy_device: NULL argument");
     Ctx& c = h->c;
     VD_CUDA(cudaSetDevice(c.device));
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c.stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the CUDA default stream
     return run_pose_kernel<0>(c, lig, n, poses, ep, e, nullptr, nullptr, nullptr, 0, s);
 }
 
