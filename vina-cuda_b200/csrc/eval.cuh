@@ -66,7 +66,7 @@ constexpr int kNdQ = 12, kNdAA = 16;
 __host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
 // Shared-memory floats one warp needs for a ligand of the given size.
 __host__ __device__ inline int warp_floats(int na, int nn, int np, int nt) {
-    return pad4(7 + nt) + kNodeF * nn + 4 * na + 3 * pad4(na) + pad4(6 * nn) + pad4(6 + nt);
+    return pad4(7 + nt) + kNodeF * nn + 4 * na + 3 * pad4(na) + 8 * nn + pad4(6 + nt);
 }
 
 struct WarpMem {
@@ -74,7 +74,7 @@ struct WarpMem {
     float* nd;
     float4* c;          // heavy-atom coordinates (w unused)
     float *fx, *fy, *fz;
-    float* ns;
+    float* ns;          // [nn][8]
     float* g;
 };
 
@@ -87,7 +87,7 @@ __device__ __forceinline__ WarpMem carve(float* p, int na, int nn, int np, int n
     m.fx = p; p += a4;
     m.fy = p; p += a4;
     m.fz = p; p += a4;
-    m.ns = p; p += pad4(6 * nn);
+    m.ns = p; p += 8 * nn;  // per body: force[3], moment[3], 2 pad (two vector loads)
     m.g = p;
     return m;
 }
@@ -290,12 +290,18 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             cur_b = nb;
             bx = by = bz = 0.f;
         };
+        float4 cb = make_float4(0.f, 0.f, 0.f, 0.f);  // coordinates of cur_b
         for (int p = p0; p < p1; p += 2) {
             const bool two = p + 1 < p1;
             const int2 q0 = __ldg(&L.pairs[p]);
             const int2 q1 = two ? __ldg(&L.pairs[p + 1]) : q0;
             const int a0 = q0.x & 0xffff, b0 = q0.x >> 16, a1 = q1.x & 0xffff, b1 = q1.x >> 16;
-            const float4 ca0 = m.c[a0], cb0 = m.c[b0], ca1 = m.c[a1], cb1 = m.c[b1];
+            if (b0 != cur_b) {  // b repeats along the segment: its coordinates stay in registers
+                flush(b0);
+                cb = m.c[b0];
+            }
+            const float4 cb0 = cb, cb1 = (b1 == b0) ? cb : m.c[b1];
+            const float4 ca0 = m.c[a0], ca1 = m.c[a1];
             const float r0x = cb0.x - ca0.x, r0y = cb0.y - ca0.y, r0z = cb0.z - ca0.z;
             const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
             const float d0 = r0x * r0x + r0y * r0y + r0z * r0z, d1 = r1x * r1x + r1y * r1y + r1z * r1z;
@@ -315,15 +321,21 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             g0 = in0 ? g0 * c0 * c0 : 0.f;
             g1 = in1 ? g1 * c1 * c1 : 0.f;
             e += e0 + e1;
+            if (!want_grad && two && b1 != cur_b) {
+                cur_b = b1;
+                cb = cb1;
+            }
             if (want_grad) {
-                if (b0 != cur_b) flush(b0);
                 if (in0) {
                     const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
                     atomicAdd(&m.fx[a0], -Fx); atomicAdd(&m.fy[a0], -Fy); atomicAdd(&m.fz[a0], -Fz);
                     bx += Fx; by += Fy; bz += Fz;
                 }
                 if (two) {
-                    if (b1 != cur_b) flush(b1);
+                    if (b1 != cur_b) {
+                        flush(b1);
+                        cb = cb1;
+                    }
                     if (in1) {
                         const float Fx = g1 * r1x, Fy = g1 * r1y, Fz = g1 * r1z;
                         atomicAdd(&m.fx[a1], -Fx); atomicAdd(&m.fy[a1], -Fy); atomicAdd(&m.fz[a1], -Fz);
@@ -341,7 +353,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     // grouped by body, so a segmented warp scan sums each body's atoms and
     // the last lane of each segment adds the result to the body.
     const float ox = m.x[0], oy = m.x[1], oz = m.x[2];
-    for (int k = lane; k < 6 * L.nn; k += 32) m.ns[k] = 0.f;
+    for (int k = lane; k < 8 * L.nn; k += 32) m.ns[k] = 0.f;
     __syncwarp();
     for (int base = 0; base < L.na; base += 32) {
         const int i = base + lane;
@@ -368,7 +380,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         }
         const int kn = __shfl_down_sync(0xffffffffu, key, 1);
         if (i < L.na && (lane == 31 || kn != key)) {
-            float* ns = m.ns + 6 * key;
+            float* ns = m.ns + 8 * key;
 #pragma unroll
             for (int j = 0; j < 6; ++j) atomicAdd(&ns[j], v[j]);
         }
@@ -379,8 +391,9 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         const int e1 = __ldg(&L.nodes[k].subtree_end);
         float F0 = 0.f, F1 = 0.f, F2 = 0.f, M0 = 0.f, M1 = 0.f, M2 = 0.f;
         for (int j = k; j < e1; ++j) {
-            const float* ns = m.ns + 6 * j;
-            F0 += ns[0]; F1 += ns[1]; F2 += ns[2]; M0 += ns[3]; M1 += ns[4]; M2 += ns[5];
+            const float4 u = *reinterpret_cast<const float4*>(m.ns + 8 * j);
+            const float2 w = *reinterpret_cast<const float2*>(m.ns + 8 * j + 4);
+            F0 += u.x; F1 += u.y; F2 += u.z; M0 += u.w; M1 += w.x; M2 += w.y;
         }
         if (k == 0) {
             m.g[0] = F0; m.g[1] = F1; m.g[2] = F2; m.g[3] = M0; m.g[4] = M1; m.g[5] = M2;
