@@ -49,6 +49,7 @@ def args_():
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--cpu-ligands", type=int, default=3, help="whole ligands in the CPU sample")
     a.add_argument("--no-configs", action="store_true", help="skip the plain / adjoint / uneven-batch lines")
+    a.add_argument("--launch-shape", type=int, default=0, help="docking kernel shape (0 = autotuned, 1-3 pinned)")
     return a.parse_args()
 
 
@@ -119,10 +120,12 @@ def lig_bytes(lig):
     return 32 * heavy + 16 * len(lig["pairs"])
 
 
-# DRAM bytes per evaluation of dock_kernel from one ncu capture of this
-# workload (profiles/dock_kernel_wide_box_screen.txt): 12.07 GB over 15.9 M
-# evaluations; the bench scales it by the evaluations of each launch.
-DOCK_DRAM_BYTES_PER_EVAL = 758.0
+# DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
+# captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
+# ligands x 6,500 chains, 11.54 M evaluations per launch): 64 registers
+# 6.31 GB, 48 registers 11.63 GB (more spills); the 40-register shape was not
+# captured.  The bench scales the figure by the evaluations of each launch.
+DOCK_DRAM_BYTES_PER_EVAL = {1: 547.0, 2: 1008.0}
 
 
 def peaks():
@@ -367,7 +370,7 @@ def run_ours(a):
     n_pts = int(np.prod(ctx.grid_dims()[0]))
     grid_bytes = 4 * n_pts * 8 + 16 * REC_ATOMS
     ids = [ctx.add_ligand(l) for l in ligs]
-    sp = vdock.search_params(seed=SEED, n_chains=a.chains, search_depth=0, refine=1)
+    sp = vdock.search_params(seed=SEED, n_chains=a.chains, search_depth=0, refine=1, launch_shape=a.launch_shape)
     batches = [ids[i * B:(i + 1) * B] for i in range(W + K)]
     for k in range(W):
         ctx.dock_batched(batches[k], sp)
@@ -384,6 +387,7 @@ def run_ours(a):
     for k in range(W, W + K):
         res = ctx.dock_batched(batches[k], sp)
         st = ctx.stats()
+        shapes = {"dock_launch_shape": st["dock_shape"], "grid_shape": st["grid_shape"]}
         dock_ms += st["dock_ms"]
         for lid, r in zip(batches[k], res):
             evals += r["bfgs_evals"]
@@ -438,7 +442,7 @@ def run_ours(a):
                    "search_depth": "heuristic (main.cpp:369)", "box_A": BOX, "receptor_atoms": REC_ATOMS,
                    "ligand_atoms": list(LIG_ATOMS), "ligand_torsions": list(LIG_TORS),
                    "parallelism": f"weak x{world} (ligand shards)",
-                   "l2": "inputs larger than L2 (8 maps x 188^3 x 4 B = 213 MB)"},
+                   "l2": "inputs larger than L2 (8 maps x 188^3 x 4 B = 213 MB)", **shapes},
         "bfgs_evals_per_s": evals * world / elapsed,
         "plain": {"value": plain_value * world, "unit": UNIT, "ligands": len(plain_ids),
                   "batched_over_plain": value / (plain_value * world)},
@@ -447,7 +451,8 @@ def run_ours(a):
                        "frac_of_hbm": grid_bytes / (min(grid_ms) / 1e3) / 1e9 / hbm},
         "roofline": {"kernel": "dock_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": DOCK_DRAM_BYTES_PER_EVAL * evals / K,
+                     "traffic": (DOCK_DRAM_BYTES_PER_EVAL[shapes["dock_launch_shape"]] * evals / K
+                                 if shapes["dock_launch_shape"] in DOCK_DRAM_BYTES_PER_EVAL else None),
                      "note": "algorithmic bytes = evals x (32 x heavy atoms + 16 x intra pairs); traffic = "
                              "ncu DRAM bytes per evaluation x evaluations per launch"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
