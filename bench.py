@@ -399,9 +399,8 @@ def run_ours(a):
     clk = clocks.stop()
     elapsed = ev0.elapsed_time(ev1) / 1e3
     if pg:
-        t = torch.tensor([elapsed], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        elapsed = float(t.item())
+        from vdock import multi
+        elapsed = multi.max_over_ranks(elapsed, device="cuda")
         pg.barrier()
     value = K * B * world / elapsed
     # plain form on a sample (one ligand per launch)
