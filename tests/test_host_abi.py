@@ -177,3 +177,18 @@ def to_pdbqt(lig):
     branches(0)
     lines.append(f"TORSDOF {len(parent) - 1}")
     return "\n".join(lines) + "\n"
+
+
+def test_autotuner_logic(tmp_path):
+    """The launch-shape autotuner (csrc/tune.h) compiled into a host check."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "tune_check"
+    src = os.path.join(REPO, "tests", "host", "tune_check.cpp")
+    inc = os.path.join(REPO, "vina-cuda_b200", "csrc")
+    subprocess.run([gxx, "-std=c++17", "-O1", "-Wall", "-I", inc, src, "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
