@@ -35,3 +35,44 @@ def test_cli_docks_reference_example(tmp_path, golden_dir):
     best = float(remarks[0].split()[3])
     assert -9.5 <= best <= -6.5, best
     assert "mode |   affinity" in r.stdout
+
+
+def test_cli_ligand_directory(tmp_path, golden_dir):
+    """--ligand_directory: every file of the directory docked in batches while
+    later files are still being parsed, outputs named <stem>_out.pdbqt in
+    --output_directory (main.cpp:897-945), unparsable files skipped with a
+    message, results independent of parse timing (two runs are identical)."""
+    if not has_gpu():
+        pytest.skip("needs a CUDA device")
+    cli = os.path.join(REPO, "vina-cuda_b200", "vdock_cli")
+    for name in ("1u1b_protein.pdbqt", "1u1b_config.txt"):
+        data = gzip.open(os.path.join(golden_dir, "pdbqt", name + ".gz"), "rb").read()
+        (tmp_path / name).write_bytes(data)
+    ligdir = tmp_path / "ligs"
+    ligdir.mkdir()
+    names = ["1u1b_ligand", "2bm2_ligand", "2er7_ligand"]
+    for name in names:
+        data = gzip.open(os.path.join(golden_dir, "pdbqt", name + ".pdbqt.gz"), "rb").read()
+        (ligdir / (name + ".pdbqt")).write_bytes(data)
+        (ligdir / (name + "_copy.pdbqt")).write_bytes(data)
+    (ligdir / "broken.pdbqt").write_text("ATOM  garbage\nBRANCH 1 2\n")
+    cfg = (tmp_path / "1u1b_config.txt").read_text()
+    lines = [l for l in cfg.splitlines() if not l.strip().startswith(("receptor", "ligand", "out", "thread"))]
+    outputs = []
+    for run in ("a", "b"):
+        lines_run = lines + ["receptor = 1u1b_protein.pdbqt", "ligand_directory = ligs", f"output_directory = out_{run}",
+                             "thread = 1000", "seed = 3", "batch = 4"]
+        (tmp_path / "cfg.txt").write_text("\n".join(lines_run) + "\n")
+        r = subprocess.run([cli, "--config", "cfg.txt"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        assert "broken.pdbqt" in r.stderr  # reported and skipped
+        assert "Docked 6 ligands" in r.stdout
+        outdir = tmp_path / f"out_{run}"
+        files = sorted(p.name for p in outdir.iterdir())
+        assert files == sorted([n + "_out.pdbqt" for n in names] + [n + "_copy_out.pdbqt" for n in names])
+        texts = {f: (outdir / f).read_text() for f in files}
+        for t in texts.values():
+            remarks = [l for l in t.splitlines() if l.startswith("REMARK VINA RESULT:")]
+            assert 1 <= len(remarks) <= 9 and float(remarks[0].split()[3]) < 0
+        outputs.append(texts)
+    assert outputs[0] == outputs[1]

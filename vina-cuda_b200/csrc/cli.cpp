@@ -2,14 +2,18 @@
 // (main.cpp:569-1020 options and config file, 89-102 write_all_output,
 // 159-170 REMARK VINA RESULT, 460-489 result table) over the C ABI.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <filesystem>
 #include <fstream>
 #include <map>
+#include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/vdock.h"
@@ -30,6 +34,80 @@ static std::string slurp(const std::string& path) {
     ss << f.rdbuf();
     return ss.str();
 }
+// Ligand files parsed on worker threads ahead of the docking loop, at most
+// `ahead` files past the consumer (bounded memory); results are consumed in
+// file order so ligand ids -- and with them the random streams -- do not
+// depend on parse timing.
+class ParsePool {
+  public:
+    struct Slot {
+        vd_pdbqt* h = nullptr;
+        vd_ligand_desc d{};
+        bool ok = false;
+        std::string err;
+    };
+    ParsePool(const std::vector<std::string>& files, size_t ahead, unsigned threads)
+        : files_(files), slots_(files.size()), ready_(files.size(), 0), ahead_(std::max<size_t>(1, ahead)) {
+        for (unsigned t = 0; t < std::max(1u, threads); ++t) th_.emplace_back([this] { work(); });
+    }
+    ~ParsePool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_space_.notify_all();
+        for (auto& t : th_) t.join();
+        for (size_t i = 0; i < slots_.size(); ++i)  // parsed but never consumed
+            if (ready_[i] && !taken_[i] && slots_[i].h) vd_pdbqt_free(slots_[i].h);
+    }
+    // Blocks until file i is parsed; the caller owns the slot's handle.
+    Slot take(size_t i) {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_ready_.wait(lk, [&] { return ready_[i] != 0; });
+        taken_[i] = 1;
+        consumed_ = i + 1;
+        cv_space_.notify_all();
+        return slots_[i];
+    }
+
+  private:
+    void work() {
+        for (;;) {
+            size_t i;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_space_.wait(lk, [&] { return stop_ || next_ >= files_.size() || next_ < consumed_ + ahead_; });
+                if (stop_ || next_ >= files_.size()) return;
+                i = next_++;
+            }
+            Slot s;
+            std::ifstream f(files_[i]);
+            if (!f) {
+                s.err = "could not open \"" + files_[i] + "\" for reading";
+            } else {
+                std::stringstream ss;
+                ss << f.rdbuf();
+                if (vd_pdbqt_ligand(ss.str().c_str(), &s.h, &s.d) == VD_OK) s.ok = true;
+                else s.err = vd_last_error();
+            }
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                slots_[i] = s;
+                ready_[i] = 1;
+            }
+            cv_ready_.notify_all();
+        }
+    }
+    std::vector<std::string> files_;
+    std::vector<Slot> slots_;
+    std::vector<char> ready_, taken_ = std::vector<char>(files_.size(), 0);
+    size_t ahead_, next_ = 0, consumed_ = 0;
+    bool stop_ = false;
+    std::mutex mu_;
+    std::condition_variable cv_ready_, cv_space_;
+    std::vector<std::thread> th_;
+};
+
 static std::string trim(std::string s) {
     while (!s.empty() && std::isspace((unsigned char)s.back())) s.pop_back();
     size_t i = 0;
@@ -96,7 +174,8 @@ int main(int argc, char** argv) {
                                num("weight_hydrogen", -0.587439), 5 * w_rot / 0.1 - 1};
 
     std::vector<std::string> ligs, outs;
-    if (opt.count("ligand")) {
+    const bool directory = opt.count("ligand_directory") != 0;
+    if (!directory) {
         ligs.push_back(opt["ligand"]);
         std::string o = opt.count("out") ? opt["out"] : opt["ligand"];
         if (!opt.count("out")) {
@@ -104,20 +183,24 @@ int main(int argc, char** argv) {
             o += "_out.pdbqt";
         }
         outs.push_back(o);
-    } else {
+    } else {  // every file of the directory (main.cpp:897-945), in name order; unparsable ones are skipped
         const std::string dir = opt["ligand_directory"];
         const std::string odir = opt.count("output_directory") ? opt["output_directory"] : dir + "_out";
         fs::create_directories(odir);
         std::vector<fs::path> files;
         for (auto& e : fs::directory_iterator(dir))
-            if (e.path().extension() == ".pdbqt") files.push_back(e.path());
+            if (e.is_regular_file()) files.push_back(e.path());
         std::sort(files.begin(), files.end());
         for (auto& f : files) {
             ligs.push_back(f.string());
-            outs.push_back((fs::path(odir) / (f.stem().string() + "_out.pdbqt")).string());
+            std::string stem = f.filename().string();
+            const size_t dot = stem.find(".pdbqt");
+            if (dot != std::string::npos) stem.resize(dot);
+            outs.push_back((fs::path(odir) / (stem + "_out.pdbqt")).string());
         }
         std::printf("Output will be in the directory %s\n", odir.c_str());
     }
+    const auto t_start = std::chrono::steady_clock::now();
 
     vd_ctx* ctx = nullptr;
     check(vd_create(&ctx, int(num("device", 0))), "vd_create");
@@ -130,35 +213,28 @@ int main(int argc, char** argv) {
     check(vd_set_receptor(ctx, nr, rxyz, rxs), "vd_set_receptor");
     check(vd_set_box(ctx, center, size), "vd_set_box");
 
-    std::vector<vd_pdbqt*> handles;
-    std::vector<vd_ligand_desc> descs;
-    std::vector<int32_t> ids;
-    std::vector<std::string> kept_out;
-    bool need[VD_XS_TYPES] = {};
-    for (size_t i = 0; i < ligs.size(); ++i) {
-        vd_pdbqt* h = nullptr;
-        vd_ligand_desc d;
-        if (vd_pdbqt_ligand(slurp(ligs[i]).c_str(), &h, &d) != VD_OK) {
-            std::fprintf(stderr, "\nParse error in file \"%s\": %s\n", ligs[i].c_str(), vd_last_error());
-            continue;
-        }
-        int32_t id = -1;
-        if (vd_add_ligand(ctx, &d, &id) != VD_OK) {
-            std::fprintf(stderr, "skipping %s: %s\n", ligs[i].c_str(), vd_last_error());
-            vd_pdbqt_free(h);
-            continue;
-        }
-        for (int a = 0; a < d.n_atoms; ++a)
-            if (d.xs[a] >= 0) need[d.xs[a]] = true;
-        handles.push_back(h);
-        descs.push_back(d);
-        ids.push_back(id);
-        kept_out.push_back(outs[i]);
-    }
-    if (ids.empty()) die("No valid ligands");
+    const int batch = std::max(1, int(num("batch", 64)));
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    ParsePool pool(ligs, size_t(4) * batch, std::min(hw, 16u));
+    // maps: a single ligand's types; for a directory all 17 (as the reference
+    // builds them, main_procedure_cu.cpp:167-175), so docking starts while
+    // later files are still being parsed
     std::vector<int32_t> types;
-    for (int t = 0; t < VD_XS_TYPES; ++t)
-        if (need[t]) types.push_back(t);
+    ParsePool::Slot first;
+    if (!directory) {
+        first = pool.take(0);
+        if (!first.ok) {
+            std::fprintf(stderr, "\nParse error in file \"%s\": %s\n", ligs[0].c_str(), first.err.c_str());
+            return 1;
+        }
+        bool need[VD_XS_TYPES] = {};
+        for (int a = 0; a < first.d.n_atoms; ++a)
+            if (first.d.xs[a] >= 0) need[first.d.xs[a]] = true;
+        for (int t = 0; t < VD_XS_TYPES; ++t)
+            if (need[t]) types.push_back(t);
+    } else {
+        for (int t = 0; t < VD_XS_TYPES; ++t) types.push_back(t);
+    }
     check(vd_build_grids(ctx, types.data(), int32_t(types.size())), "vd_build_grids");
 
     vd_search_params sp{};
@@ -173,42 +249,74 @@ int main(int argc, char** argv) {
     sp.amplitude = 2.0;
     sp.min_rmsd = 1.0;
     sp.refine = 1;
-    std::vector<vd_dock_result> res(ids.size());
-    const int batch = std::max(1, int(num("batch", 64)));
-    for (size_t b = 0; b < ids.size(); b += batch) {
-        const int n = int(std::min(ids.size() - b, size_t(batch)));
-        if (n == 1) check(vd_dock_plain(ctx, ids[b], &sp, &res[b]), "vd_dock_plain");
-        else check(vd_dock_batched(ctx, &ids[b], n, &sp, &res[b]), "vd_dock_batched");
-    }
     FILE* log = opt.count("log") ? std::fopen(opt["log"].c_str(), "w") : nullptr;
-    for (size_t i = 0; i < ids.size(); ++i) {
-        const vd_dock_result& r = res[i];
-        std::string table = "mode |   affinity | dist from best mode\n     | (kcal/mol) | rmsd l.b.| rmsd u.b.\n"
-                            "-----+------------+----------+----------\n";
-        std::ofstream f(kept_out[i]);
-        if (!f) die("could not open \"" + kept_out[i] + "\" for writing.");
-        std::vector<double> xyz(3 * size_t(descs[i].n_atoms));
-        for (int m = 0; m < r.n_modes; ++m) {
-            char line[128];
-            std::snprintf(line, sizeof line, "%4d    %9.1f  %9.3f  %9.3f\n", m + 1, r.energy[m], r.rmsd_lb[m], r.rmsd_ub[m]);
-            table += line;
-            check(vd_conf_to_coords(&descs[i], r.pose[m], xyz.data()), "vd_conf_to_coords");
-            int64_t len = 0;
-            check(vd_pdbqt_write_model(handles[i], xyz.data(), nullptr, 0, &len), "write");
-            std::string buf(size_t(len) + 1, '\0');
-            check(vd_pdbqt_write_model(handles[i], xyz.data(), &buf[0], len + 1, &len), "write");
-            char remark[128];
-            std::snprintf(remark, sizeof remark, "REMARK VINA RESULT: %9.1f  %9.3f  %9.3f\n", r.energy[m], r.rmsd_lb[m],
-                          r.rmsd_ub[m]);
-            f << "MODEL " << m + 1 << "\n" << remark << buf.c_str() << "ENDMDL\n";
+
+    struct Item {
+        size_t file;
+        ParsePool::Slot s;
+        int32_t id;
+    };
+    std::vector<Item> pending;
+    size_t n_docked = 0;
+    auto run_batch = [&]() {
+        std::vector<int32_t> ids;
+        for (auto& it : pending) ids.push_back(it.id);
+        std::vector<vd_dock_result> res(ids.size());
+        if (ids.size() == 1) check(vd_dock_plain(ctx, ids[0], &sp, &res[0]), "vd_dock_plain");
+        else check(vd_dock_batched(ctx, ids.data(), int32_t(ids.size()), &sp, res.data()), "vd_dock_batched");
+        for (size_t k = 0; k < pending.size(); ++k) {
+            const Item& it = pending[k];
+            const vd_dock_result& r = res[k];
+            const std::string& out = outs[it.file];
+            std::string table = "mode |   affinity | dist from best mode\n     | (kcal/mol) | rmsd l.b.| rmsd u.b.\n"
+                                "-----+------------+----------+----------\n";
+            std::ofstream f(out);
+            if (!f) die("could not open \"" + out + "\" for writing.");
+            std::vector<double> xyz(3 * size_t(it.s.d.n_atoms));
+            for (int m = 0; m < r.n_modes; ++m) {
+                char line[128];
+                std::snprintf(line, sizeof line, "%4d    %9.1f  %9.3f  %9.3f\n", m + 1, r.energy[m], r.rmsd_lb[m],
+                              r.rmsd_ub[m]);
+                table += line;
+                check(vd_conf_to_coords(&it.s.d, r.pose[m], xyz.data()), "vd_conf_to_coords");
+                int64_t len = 0;
+                check(vd_pdbqt_write_model(it.s.h, xyz.data(), nullptr, 0, &len), "write");
+                std::string buf(size_t(len) + 1, '\0');
+                check(vd_pdbqt_write_model(it.s.h, xyz.data(), &buf[0], len + 1, &len), "write");
+                char remark[128];
+                std::snprintf(remark, sizeof remark, "REMARK VINA RESULT: %9.1f  %9.3f  %9.3f\n", r.energy[m],
+                              r.rmsd_lb[m], r.rmsd_ub[m]);
+                f << "MODEL " << m + 1 << "\n" << remark << buf.c_str() << "ENDMDL\n";
+            }
+            if (r.n_modes < 1)
+                table += "WARNING: Could not find any conformations completely within the search space.\n";
+            std::printf("%s\n%s", directory ? out.c_str() : "", table.c_str());
+            if (log) std::fprintf(log, "%s", table.c_str());
+            vd_pdbqt_free(it.s.h);
         }
-        if (r.n_modes < 1)
-            table += "WARNING: Could not find any conformations completely within the search space.\n";
-        std::printf("%s\n%s", ligs.size() > 1 ? kept_out[i].c_str() : "", table.c_str());
-        if (log) std::fprintf(log, "%s", table.c_str());
+        n_docked += pending.size();
+        pending.clear();
+    };
+    for (size_t i = 0; i < ligs.size(); ++i) {
+        ParsePool::Slot s = (i == 0 && !directory) ? first : pool.take(i);
+        if (!s.ok) {
+            std::fprintf(stderr, "\nParse error in file \"%s\": %s\n", ligs[i].c_str(), s.err.c_str());
+            continue;
+        }
+        int32_t id = -1;
+        if (vd_add_ligand(ctx, &s.d, &id) != VD_OK) {
+            std::fprintf(stderr, "skipping %s: %s\n", ligs[i].c_str(), vd_last_error());
+            vd_pdbqt_free(s.h);
+            continue;
+        }
+        pending.push_back({i, s, id});
+        if (int(pending.size()) == batch) run_batch();
     }
+    if (!pending.empty()) run_batch();
+    if (n_docked == 0) die(directory ? "No valid ligands in the input directory" : "No valid ligands");
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (directory) std::printf("Docked %zu ligands in %.2f s\n", n_docked, secs);
     if (log) std::fclose(log);
-    for (auto* h : handles) vd_pdbqt_free(h);
     vd_pdbqt_free(rh);
     vd_destroy(ctx);
     return 0;

@@ -132,7 +132,8 @@ struct Ctx {
     // ligands
     std::vector<HostLigand> ligs;
     float4* d_pool = nullptr;
-    int64_t pool_words = 0, pool_cap = 0;
+    int64_t pool_words = 0, pool_cap = 0;   // words of all added ligands / device capacity
+    size_t pool_synced = 0;                 // ligands already on the device
     bool pool_dirty = false;
     // scratch
     void* d_scratch = nullptr;

@@ -8,28 +8,42 @@
 
 namespace vd {
 
+// Uploads the ligands added since the last call.  Offsets are fixed when a
+// ligand is added, so the upload is append-only: only new blobs cross PCIe
+// (growing the buffer copies the old contents device to device).
 vd_status sync_pool(Ctx* c) {
     if (!c->pool_dirty) return VD_OK;
-    int64_t words = 0;
-    for (auto& L : c->ligs) words += int64_t(L.blob.size());
-    if (words > c->pool_cap) {
+    const int64_t words = c->pool_words;
+    if (words > c->pool_cap || !c->d_pool) {
+        const int64_t cap = std::max<int64_t>(words + words / 2, 4096);
+        float4* fresh = nullptr;
+        VD_CUDA(cudaMalloc(&fresh, size_t(cap) * sizeof(float4)));
+        int64_t keep = 0;
+        if (c->pool_synced > 0) {
+            const HostLigand& last = c->ligs[c->pool_synced - 1];
+            keep = last.pool_offset + int64_t(last.blob.size());
+        }
+        if (c->d_pool && keep > 0)
+            VD_CUDA(cudaMemcpyAsync(fresh, c->d_pool, size_t(keep) * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                    c->stream));
+        VD_CUDA(cudaStreamSynchronize(c->stream));
         if (c->d_pool) VD_CUDA(cudaFree(c->d_pool));
-        c->d_pool = nullptr;
-        int64_t cap = std::max<int64_t>(words + words / 2, 4096);
-        VD_CUDA(cudaMalloc(&c->d_pool, size_t(cap) * sizeof(float4)));
+        c->d_pool = fresh;
         c->pool_cap = cap;
     }
-    std::vector<float4> host(size_t(std::max<int64_t>(words, 1)));
-    int64_t off = 0;
-    for (auto& L : c->ligs) {
-        L.pool_offset = off;
-        std::memcpy(&host[size_t(off)], L.blob.data(), L.blob.size() * sizeof(float4));
-        off += int64_t(L.blob.size());
+    const size_t first = c->pool_synced;
+    if (first < c->ligs.size()) {
+        const int64_t begin = c->ligs[first].pool_offset;
+        std::vector<float4> host(size_t(words - begin));
+        for (size_t i = first; i < c->ligs.size(); ++i) {
+            const HostLigand& L = c->ligs[i];
+            std::memcpy(&host[size_t(L.pool_offset - begin)], L.blob.data(), L.blob.size() * sizeof(float4));
+        }
+        VD_CUDA(cudaMemcpyAsync(c->d_pool + begin, host.data(), host.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                                c->stream));
+        VD_CUDA(cudaStreamSynchronize(c->stream));
     }
-    VD_CUDA(cudaMemcpyAsync(c->d_pool, host.data(), size_t(words) * sizeof(float4), cudaMemcpyHostToDevice,
-                            c->stream));
-    VD_CUDA(cudaStreamSynchronize(c->stream));
-    c->pool_words = words;
+    c->pool_synced = c->ligs.size();
     c->pool_dirty = false;
     return VD_OK;
 }
@@ -197,6 +211,8 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     L.heavy_index = heavy_index;
     L.n_all_atoms = na;
     L.num_tors = d->num_tors;
+    L.pool_offset = c.pool_words;
+    c.pool_words += int64_t(L.blob.size());
     c.ligs.push_back(std::move(L));
     c.pool_dirty = true;
     *lig_id = int32_t(c.ligs.size()) - 1;
@@ -215,6 +231,8 @@ vd_status vd_ligand_info(vd_ctx* h, int32_t lig, int32_t* n_heavy, int32_t* ntor
 vd_status vd_clear_ligands(vd_ctx* h) {
     VD_CHECK(h, VD_ERR_ARG, "vd_clear_ligands: NULL context");
     h->c.ligs.clear();
+    h->c.pool_words = 0;
+    h->c.pool_synced = 0;
     h->c.pool_dirty = true;
     return VD_OK;
 }
