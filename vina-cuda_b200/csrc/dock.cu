@@ -56,8 +56,7 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
 }
 
 // MINB: 4-warp blocks per SM the register budget targets (8/10/12 -> 64/48/40
-// registers per thread; the 40-register build takes one intra pair per loop
-// iteration, the others two); the autotuner picks one per workload.
+// registers per thread); the autotuner picks one per workload.
 template <bool persistent, int MINB>
 __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
     extern __shared__ float4 smem4[];
@@ -96,7 +95,7 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
             // pass 0 optimises the candidate; pass 1 re-optimises an accepted
             // candidate that beats the chain's best (one optimiser call site)
             for (int pass = 0; pass < 2; ++pass) {
-                const float ce = rilc_bfgs<(MINB >= 12) ? 1 : 2>(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
+                const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
                 if (pass == 0) {
                     const bool accept = step == 0 || ce < tmp_e ||
                                         u01(b[1]) < __expf((tmp_e - ce) / p.temperature);  // kernel2.cu:63-71

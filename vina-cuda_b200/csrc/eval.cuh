@@ -260,10 +260,7 @@ struct GridInter {
     }
 };
 
-// kPairs: intra pairs per loop iteration (2 keeps two table gathers in
-// flight; 1 needs fewer registers).  Both sum the pair energies in the same
-// pairwise grouping, so their results are bit-identical.
-template <bool want_grad, class Inter, int kPairs = 2>
+template <bool want_grad, class Inter>
 __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const Inter& inter, const float4* smooth,
                              float v_intra, int lane) {
     kinematics(L, m, lane);
@@ -294,7 +291,6 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             bx = by = bz = 0.f;
         };
         float4 cb = make_float4(0.f, 0.f, 0.f, 0.f);  // coordinates of cur_b
-        if constexpr (kPairs == 2) {
         for (int p = p0; p < p1; p += 2) {
             const bool two = p + 1 < p1;
             const int2 q0 = __ldg(&L.pairs[p]);
@@ -347,40 +343,6 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
                     }
                 }
             }
-        }
-        } else {
-            float pend = 0.f;  // energy of an unpaired pair, added as (pend + e0) like two at a time
-            bool odd = false;
-            for (int p = p0; p < p1; ++p) {
-                const int2 q0 = __ldg(&L.pairs[p]);
-                const int a0 = q0.x & 0xffff, b0 = q0.x >> 16;
-                if (b0 != cur_b) {
-                    flush(b0);
-                    cb = m.c[b0];
-                }
-                const float4 ca0 = m.c[a0];
-                const float r0x = cb.x - ca0.x, r0y = cb.y - ca0.y, r0z = cb.z - ca0.z;
-                const float d0 = r0x * r0x + r0y * r0y + r0z * r0z;
-                const float rf0 = fminf(32.f * d0, 2047.5f);
-                const int i0 = int(rf0);
-                const bool in0 = d0 < 64.f;
-                float4 t0 = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (in0) t0 = __ldg(smooth + size_t(q0.y) * kBins + i0);
-                const float w0 = rf0 - float(i0);
-                float e0 = t0.x + w0 * (t0.z - t0.x), g0 = t0.y + w0 * (t0.w - t0.y);
-                const float c0 = (e0 > 0.f) ? __fdividef(v_intra, v_intra + e0) : 1.f;
-                e0 = in0 ? e0 * c0 : 0.f;
-                g0 = in0 ? g0 * c0 * c0 : 0.f;
-                if (odd) e += pend + e0;
-                else pend = e0;
-                odd = !odd;
-                if (want_grad && in0) {
-                    const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
-                    atomicAdd(&m.fx[a0], -Fx); atomicAdd(&m.fy[a0], -Fy); atomicAdd(&m.fz[a0], -Fz);
-                    bx += Fx; by += Fy; bz += Fz;
-                }
-            }
-            if (odd) e += pend + 0.f;
         }
         flush(-1);
     }
@@ -453,11 +415,11 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     return e;
 }
 
-template <bool want_grad, int kPairs = 2>
+template <bool want_grad>
 __device__ __forceinline__ float eval_pose(const LigView& L, const WarpMem& m, const MapView& G,
                                            const float4* smooth, const EvalParams ep, int lane) {
     const GridInter gi{&G, ep.v_inter, ep.slope};
-    return eval_pose_t<want_grad, GridInter, kPairs>(L, m, gi, smooth, ep.v_intra, lane);
+    return eval_pose_t<want_grad>(L, m, gi, smooth, ep.v_intra, lane);
 }
 
 }  // namespace vd
