@@ -107,3 +107,24 @@ def test_batched_pipeline_replays_one_graph(vd):
     assert ctx.stats()["graph_launches"] == s1["graph_launches"]
     for a, b in zip(plain, ref):
         assert np.array_equal(a["energy"], b["energy"]) and np.array_equal(a["pose"], b["pose"])
+
+
+def test_shapes_bit_identical_on_screen_sized_ligands(vd):
+    """The same on ligands of the wide-box screen's size (30-45 heavy atoms,
+    up to ~700 intra pairs) with the heuristic search depth: every result
+    and every ligand's evaluation count agree across the three shapes."""
+    from vdock import synth
+    xyz, xs = synth.receptor(2000, 30.0, 8)
+    ctx = vd.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0.0, 0.0, 0.0], [24.0] * 3)
+    ctx.build_grids(synth.TYPES8)
+    ligs = [ctx.add_ligand(l) for l in synth.ligand_set(6, (30, 45), (6, 12), 17)]
+    outs = []
+    for shape in (1, 2, 3):
+        sp = vd.search_params(seed=9, n_chains=1000, search_depth=0, refine=1, launch_shape=shape)
+        outs.append(ctx.dock_batched(ligs, sp))
+    for res in outs[1:]:
+        for a, b in zip(res, outs[0]):
+            assert a["bfgs_evals"] == b["bfgs_evals"]
+            assert np.array_equal(a["energy"], b["energy"]) and np.array_equal(a["pose"], b["pose"])
