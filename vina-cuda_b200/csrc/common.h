@@ -77,7 +77,7 @@ struct NodeRec {
     int32_t atom_end;
     int32_t subtree_end;  // nodes [k, subtree_end) form k's subtree
     int32_t depth;
-    int32_t pad;
+    int32_t sub_atom_end;  // heavy atoms [atom_begin, sub_atom_end) belong to k's subtree
 };
 static_assert(sizeof(NodeRec) == 48, "node size");
 

@@ -10,10 +10,13 @@
 //      per iteration: intra pair term; the force on the second atom is
 //      accumulated in registers, the force on the first atom is added with a
 //      shared-memory atomic (model.cpp:1241-1256)
-//   6. lanes = bodies: own force and moment about the root origin
-//   7. lanes = bodies: subtree sums over the pre-order range [k, end_k),
-//        torque T_k = M_k - (o_k - o_root) x F_k, dE/dtorsion = T_k . axis_k
-//      (the bottom-up recursion of tree.h:169-178, 341-348, 373-422)
+//   6. lanes = contiguous atom ranges: warp prefix sums over the heavy atoms
+//      of force and moment about the root origin
+//   7. lanes = bodies: subtree sums as differences of two prefixes (a
+//        subtree's atoms are one contiguous range: atoms are grouped by body
+//        in pre-order), torque T_k = M_k - (o_k - o_root) x F_k,
+//        dE/dtorsion = T_k . axis_k (the bottom-up recursion of
+//        tree.h:169-178, 341-348, 373-422)
 //   8. warp butterfly sum of the energy (deterministic).
 // The per-body and subtree sums run in a fixed order; the pair-force
 // atomics are issued in a fixed program order by a single warp.
@@ -66,7 +69,7 @@ constexpr int kNdQ = 12, kNdAA = 16;
 __host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
 // Shared-memory floats one warp needs for a ligand of the given size.
 __host__ __device__ inline int warp_floats(int na, int nn, int np, int nt) {
-    return pad4(7 + nt) + kNodeF * nn + 4 * na + 3 * pad4(na) + 8 * nn + pad4(6 + nt);
+    return pad4(7 + nt) + kNodeF * nn + 4 * na + 3 * pad4(na) + 3 * pad4(na) + pad4(6 + nt);
 }
 
 struct WarpMem {
@@ -74,7 +77,7 @@ struct WarpMem {
     float* nd;
     float4* c;          // heavy-atom coordinates (w unused)
     float *fx, *fy, *fz;
-    float* ns;          // [nn][8]
+    float* ns;          // [3][pad4(na)] prefix moments
     float* g;
 };
 
@@ -87,7 +90,7 @@ __device__ __forceinline__ WarpMem carve(float* p, int na, int nn, int np, int n
     m.fx = p; p += a4;
     m.fy = p; p += a4;
     m.fz = p; p += a4;
-    m.ns = p; p += 8 * nn;  // per body: force[3], moment[3], 2 pad (two vector loads)
+    m.ns = p; p += 3 * pad4(na);  // prefix moments [3][pad4(na)] (prefix forces overwrite fx/fy/fz)
     m.g = p;
     return m;
 }
@@ -232,22 +235,6 @@ __device__ __forceinline__ float grid_term(const MapView& G, const float* map, f
     return f + penalty;
 }
 
-// Intra pair term from the smooth table (precalculate.h:80-95), curl with v.
-__device__ __forceinline__ float pair_term(const float4* smooth, int tp, float r2, float v, float& dor) {
-    const float rf = 32.f * r2;
-    const int i1 = int(rf);
-    const float rem = rf - float(i1);
-    const float4 t = __ldg(smooth + size_t(tp) * kBins + i1);
-    float e = t.x + rem * (t.z - t.x);
-    dor = t.y + rem * (t.w - t.y);
-    if (e > 0.f) {
-        const float c = __fdividef(v, v + e);
-        e *= c;
-        dor *= c * c;
-    }
-    return e;
-}
-
 // Energy (and, when want_grad, the gradient into m.g) of the pose in m.x.
 // Returns the same value in every lane.
 // Inter-molecular term of one atom on the cached grid maps.
@@ -349,18 +336,18 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     e = warp_sum(e);
     if (!want_grad) return e;
     __syncwarp();
-    // 6: own force and moment about the root origin per body.  Atoms are
-    // grouped by body, so a segmented warp scan sums each body's atoms and
-    // the last lane of each segment adds the result to the body.
+    // 6: prefix sums over the heavy atoms of force and moment about the root
+    // origin.  Atoms are grouped by body in pre-order, so a subtree's atoms
+    // are one contiguous range and its sums are a difference of two prefixes.
+    // Lane l owns atoms [l*A, l*A + A); prefix forces overwrite fx/fy/fz.
     const float ox = m.x[0], oy = m.x[1], oz = m.x[2];
-    for (int k = lane; k < 8 * L.nn; k += 32) m.ns[k] = 0.f;
-    __syncwarp();
-    for (int base = 0; base < L.na; base += 32) {
-        const int i = base + lane;
-        int key = -1 - lane;
-        float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (i < L.na) {
-            key = (__float_as_int(__ldg(&L.atoms[i].w)) >> 8) & 0xff;
+    {
+        const int A = (L.na + 31) >> 5, a0 = lane * A, a1 = min(L.na, a0 + A);
+        const int a4 = pad4(L.na);
+        float* mx = m.ns;
+        float* my = m.ns + a4;
+        float* mz = m.ns + 2 * a4;
+        auto contrib = [&](int i, float v[6]) {
             const float4 ci = m.c[i];
             const float fx = m.fx[i], fy = m.fy[i], fz = m.fz[i];
             const float dx = ci.x - ox, dy = ci.y - oy, dz = ci.z - oz;
@@ -368,32 +355,52 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             v[3] = dy * fz - dz * fy;
             v[4] = dz * fx - dx * fz;
             v[5] = dx * fy - dy * fx;
+        };
+        float run[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int i = a0; i < a1; ++i) {
+            float v[6];
+            contrib(i, v);
+#pragma unroll
+            for (int j = 0; j < 6; ++j) run[j] += v[j];
         }
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const int ko = __shfl_up_sync(0xffffffffu, key, off);
+        for (int off = 1; off < 32; off <<= 1) {  // inclusive scan of the lane totals
 #pragma unroll
             for (int j = 0; j < 6; ++j) {
-                const float o = __shfl_up_sync(0xffffffffu, v[j], off);
-                if (lane >= off && ko == key) v[j] += o;
+                const float o = __shfl_up_sync(0xffffffffu, run[j], off);
+                if (lane >= off) run[j] += o;
             }
         }
-        const int kn = __shfl_down_sync(0xffffffffu, key, 1);
-        if (i < L.na && (lane == 31 || kn != key)) {
-            float* ns = m.ns + 8 * key;
+        float acc[6];
 #pragma unroll
-            for (int j = 0; j < 6; ++j) atomicAdd(&ns[j], v[j]);
+        for (int j = 0; j < 6; ++j) acc[j] = __shfl_up_sync(0xffffffffu, run[j], 1);
+        if (lane == 0)
+#pragma unroll
+            for (int j = 0; j < 6; ++j) acc[j] = 0.f;
+        for (int i = a0; i < a1; ++i) {
+            float v[6];
+            contrib(i, v);
+#pragma unroll
+            for (int j = 0; j < 6; ++j) acc[j] += v[j];
+            m.fx[i] = acc[0]; m.fy[i] = acc[1]; m.fz[i] = acc[2];
+            mx[i] = acc[3]; my[i] = acc[4]; mz[i] = acc[5];
         }
     }
     __syncwarp();
-    // 7: subtree sums, torques and the pose gradient
+    // 7: subtree sums (prefix differences), torques and the pose gradient
     for (int k = lane; k < L.nn; k += 32) {
-        const int e1 = __ldg(&L.nodes[k].subtree_end);
+        const int b = __ldg(&L.nodes[k].atom_begin), e1 = __ldg(&L.nodes[k].sub_atom_end);
+        const int a4 = pad4(L.na);
         float F0 = 0.f, F1 = 0.f, F2 = 0.f, M0 = 0.f, M1 = 0.f, M2 = 0.f;
-        for (int j = k; j < e1; ++j) {
-            const float4 u = *reinterpret_cast<const float4*>(m.ns + 8 * j);
-            const float2 w = *reinterpret_cast<const float2*>(m.ns + 8 * j + 4);
-            F0 += u.x; F1 += u.y; F2 += u.z; M0 += u.w; M1 += w.x; M2 += w.y;
+        if (e1 > b) {
+            const int hi = e1 - 1;
+            F0 = m.fx[hi]; F1 = m.fy[hi]; F2 = m.fz[hi];
+            M0 = m.ns[hi]; M1 = m.ns[a4 + hi]; M2 = m.ns[2 * a4 + hi];
+            if (b > 0) {
+                const int lo = b - 1;
+                F0 -= m.fx[lo]; F1 -= m.fy[lo]; F2 -= m.fz[lo];
+                M0 -= m.ns[lo]; M1 -= m.ns[a4 + lo]; M2 -= m.ns[2 * a4 + lo];
+            }
         }
         if (k == 0) {
             m.g[0] = F0; m.g[1] = F1; m.g[2] = F2; m.g[3] = M0; m.g[4] = M1; m.g[5] = M2;

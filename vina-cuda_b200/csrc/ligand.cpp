@@ -186,8 +186,16 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
         std::memcpy(&a.w, &packed, sizeof(int));
         atoms[hi] = a;
     }
-    for (auto& r : nodes)
-        if (r.atom_begin > r.atom_end) r.atom_begin = r.atom_end = 0;
+    // heavy atoms are grouped by body in pre-order: body k owns [hb[k], hb[k+1])
+    // and its subtree [hb[k], hb[subtree_end])
+    std::vector<int> hb(nn + 1, 0);
+    for (int hi = 0; hi < nh; ++hi) ++hb[d->atom_node[heavy_index[hi]] + 1];
+    for (int k = 0; k < nn; ++k) hb[k + 1] += hb[k];
+    for (int k = 0; k < nn; ++k) {
+        nodes[k].atom_begin = hb[k];
+        nodes[k].atom_end = hb[k + 1];
+        nodes[k].sub_atom_end = hb[sub_end[k]];
+    }
     HostLigand L;
     LigHeader& H = L.h;
     std::memset(&H, 0, sizeof(H));
