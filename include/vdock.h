@@ -114,6 +114,7 @@ typedef struct {
                                     per 256 threads, 2 = 16x8x4 per 128         */
     int64_t graph_launches;      /* batched pipelines submitted as a CUDA graph */
     int64_t graph_instantiations;/* executables built (the rest were updated in place) */
+    double  scoring_ms;          /* wall time of the last vd_set_scoring(_device) */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -126,6 +127,12 @@ vd_status vd_get_stats(vd_ctx* ctx, vd_stats* out);
 /* weights: gauss1, gauss2, repulsion, hydrophobic, hydrogen, and the internal
  * rotor weight 5*w_rot/0.1-1 (main.cpp:862). */
 vd_status vd_set_scoring(vd_ctx* ctx, const double weights[6]);
+/* Same, with the tables built on the GPU (one thread per table entry) for
+ * weight sweeps: the host build takes milliseconds per weight set.  The
+ * arithmetic and order are the host's; only exp() may differ by an ulp, so
+ * tables agree with vd_set_scoring's to ~1e-15 relative (precalculate.h:255-283
+ * on the device; no reference counterpart as an entry point). */
+vd_status vd_set_scoring_device(vd_ctx* ctx, const double weights[6]);
 vd_status vd_set_receptor(vd_ctx* ctx, int32_t n_atoms, const double* xyz, const int32_t* xs);
 vd_status vd_set_box(vd_ctx* ctx, const double center[3], const double size[3]);
 vd_status vd_grid_dims(vd_ctx* ctx, int32_t npts[3], double begin[3], double end[3]);

@@ -1,5 +1,6 @@
 // Context lifetime, errors, scoring tables, receptor and box set-up.
 #include <cmath>
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -106,9 +107,18 @@ vd_status vd_get_stats(vd_ctx* h, vd_stats* out) {
     return VD_OK;
 }
 
+// After new tables: maps built with the old weights are stale.
+static void scoring_changed(Ctx& c, std::chrono::steady_clock::time_point t0) {
+    c.scoring = true;
+    c.n_maps = 0;
+    for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
+    c.stats.scoring_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 vd_status vd_set_scoring(vd_ctx* h, const double weights[6]) {
     VD_CHECK(h && weights, VD_ERR_ARG, "vd_set_scoring: NULL argument");
     Ctx& c = h->c;
+    const auto t0 = std::chrono::steady_clock::now();
     VD_CUDA(cudaSetDevice(c.device));
     std::memcpy(c.weights, weights, sizeof(c.weights));
     build_tables(weights, c.fast, c.se, c.sd);
@@ -130,10 +140,19 @@ vd_status vd_set_scoring(vd_ctx* h, const double weights[6]) {
     VD_CUDA(cudaMemcpy(c.d_fastd, fd.data(), fd.size() * sizeof(double), cudaMemcpyHostToDevice));
     VD_CUDA(cudaMemcpy(c.d_fast, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
     VD_CUDA(cudaMemcpy(c.d_smooth, s.data(), s.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    c.scoring = true;
-    // maps depend on the weights
-    c.n_maps = 0;
-    for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
+    scoring_changed(c, t0);
+    return VD_OK;
+}
+
+vd_status vd_set_scoring_device(vd_ctx* h, const double weights[6]) {
+    VD_CHECK(h && weights, VD_ERR_ARG, "vd_set_scoring_device: NULL argument");
+    Ctx& c = h->c;
+    const auto t0 = std::chrono::steady_clock::now();
+    VD_CUDA(cudaSetDevice(c.device));
+    std::memcpy(c.weights, weights, sizeof(c.weights));
+    vd_status st = build_tables_device(c, weights);
+    if (st != VD_OK) return st;
+    scoring_changed(c, t0);
     return VD_OK;
 }
 

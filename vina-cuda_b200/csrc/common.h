@@ -166,6 +166,9 @@ vd_status sync_pool(Ctx* c);
 vd_status ensure_receptor_cells(Ctx* c);
 void build_tables(const double w[6], std::vector<double>& fast, std::vector<double>& se,
                   std::vector<double>& sd);
+// Same tables built on the device into the context's device copies, with
+// the double tables copied back to c.fast / c.se / c.sd.
+vd_status build_tables_device(Ctx& c, const double w[6]);
 
 }  // namespace vd
 

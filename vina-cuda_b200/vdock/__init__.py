@@ -55,11 +55,12 @@ class Stats(C.Structure):
     _fields_ = [("bfgs_evals", C.c_int64), ("grid_ms", C.c_double), ("dock_ms", C.c_double),
                 ("post_ms", C.c_double), ("dock_warps_per_block", C.c_int32), ("dock_blocks", C.c_int32),
                 ("dock_shape", C.c_int32), ("grid_shape", C.c_int32), ("graph_launches", C.c_int64),
-                ("graph_instantiations", C.c_int64)]
+                ("graph_instantiations", C.c_int64), ("scoring_ms", C.c_double)]
 
 
 EXPORTS = [
-    "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_scoring", "vd_set_receptor",
+    "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_scoring", "vd_set_scoring_device",
+    "vd_set_receptor",
     "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
     "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
     "vd_pose_coords",
@@ -80,6 +81,7 @@ def lib():
         L.vd_destroy.argtypes = [_vp]
         L.vd_get_stats.argtypes = [_vp, C.POINTER(Stats)]
         L.vd_set_scoring.argtypes = [_vp, _dp]
+        L.vd_set_scoring_device.argtypes = [_vp, _dp]
         L.vd_set_receptor.argtypes = [_vp, C.c_int32, _dp, _ip]
         L.vd_set_box.argtypes = [_vp, _dp, _dp]
         L.vd_grid_dims.argtypes = [_vp, _ip, _dp, _dp]
@@ -103,7 +105,8 @@ def lib():
         L.vd_refine.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.c_int32, _fp]
         L.vd_score.argtypes = [_vp, C.c_int32, C.c_int32, _fp, _fp, _fp]
         L.vd_get_tables.argtypes = [_vp, _dp, _dp, _dp]
-        for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_scoring", "vd_set_receptor",
+        for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_scoring", "vd_set_scoring_device",
+                     "vd_set_receptor",
                      "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand",
                      "vd_ligand_info", "vd_clear_ligands", "vd_energy", "vd_energy_grad",
                      "vd_energy_grad_device", "vd_energy_device", "vd_pose_coords", "vd_local_opt",
@@ -182,6 +185,13 @@ class Context:
         s = Stats()
         _check(self.L.vd_get_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def set_scoring(self, weights, device=False):
+        """New scoring weights (gauss1, gauss2, repulsion, hydrophobic, hydrogen,
+        rotor); device=True builds the tables on the GPU."""
+        w, wp = _d(np.asarray(weights, dtype=np.float64))
+        fn = self.L.vd_set_scoring_device if device else self.L.vd_set_scoring
+        _check(fn(self.h, wp))
 
     def tables(self):
         n = 153 * 2051
