@@ -192,3 +192,87 @@ def test_autotuner_logic(tmp_path):
     subprocess.run([gxx, "-std=c++17", "-O1", "-Wall", "-I", inc, src, "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
+def _mutate(lines, rng):
+    keys = ["ROOT", "ENDROOT", "BRANCH   1   2", "ENDBRANCH   1   2", "TORSDOF 3", "MODEL 1", "ENDMDL", "BRANCH",
+            "BRANCH 9999 1", "ENDBRANCH 5 5", ""]
+    lines = list(lines)
+    for _ in range(rng.randint(1, 6)):
+        if not lines:
+            lines = [""]
+        op, i = rng.randint(0, 7), rng.randrange(len(lines))
+        if op == 0:
+            del lines[i]
+        elif op == 1:
+            lines.insert(i, lines[rng.randrange(len(lines))])
+        elif op == 2:
+            j = rng.randrange(len(lines))
+            lines[i], lines[j] = lines[j], lines[i]
+        elif op == 3:
+            lines[i] = lines[i][:rng.randint(0, len(lines[i]))]
+        elif op == 4:
+            chars = list(lines[i])
+            for _ in range(rng.randint(1, 5)):
+                if chars:
+                    chars[rng.randrange(len(chars))] = rng.choice("0123456789.-+ eEXx\t#ABZ")
+            lines[i] = "".join(chars)
+        elif op == 5:
+            lines.insert(i, rng.choice(keys))
+        elif op == 6:
+            lines[i] += " " * rng.randint(0, 40) + rng.choice(["1e308", "nan", "inf", "-0", "99999999"])
+        else:
+            lines[i] = "".join(chr(rng.randint(1, 126)) for _ in range(rng.randint(0, 90)))
+    return lines
+
+
+def test_parser_survives_mutated_inputs(lib, golden_dir):
+    """PDBQT input is untrusted: 2,000 randomly mutated ligand and receptor
+    files (deleted, duplicated, swapped, truncated and garbled lines, stray
+    ROOT/BRANCH/TORSDOF/MODEL records, huge or non-finite numbers) must each
+    parse or fail with VD_ERR_PARSE, never crash; every ligand that parses
+    goes through the host kinematics and the PDBQT writer."""
+    import random
+    import vdock
+    lib.vd_pdbqt_ligand.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(vdock.LigandDesc)]
+    lib.vd_pdbqt_ligand.restype = C.c_int
+    lib.vd_pdbqt_receptor.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int32),
+                                      C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.POINTER(C.c_int32))]
+    lib.vd_pdbqt_receptor.restype = C.c_int
+    lib.vd_conf_to_coords.argtypes = [C.POINTER(vdock.LigandDesc), C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    lib.vd_conf_to_coords.restype = C.c_int
+    lib.vd_pdbqt_write_model.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.c_char_p, C.c_int64,
+                                         C.POINTER(C.c_int64)]
+    lib.vd_pdbqt_write_model.restype = C.c_int
+    lib.vd_pdbqt_free.argtypes = [C.c_void_p]
+    ligs = [fixture_text(golden_dir, n).splitlines() for n in ("1u1b_ligand.pdbqt", "2bm2_ligand.pdbqt",
+                                                             "2er7_ligand.pdbqt")]
+    rec = fixture_text(golden_dir, "1u1b_protein.pdbqt").splitlines()[:400]
+    rng = random.Random(20261203)
+    seen = {0: 0, 5: 0}
+    for _ in range(2000):
+        if rng.random() < 0.8:
+            text = "\n".join(_mutate(rng.choice(ligs), rng))
+            h, d = C.c_void_p(), vdock.LigandDesc()
+            st = lib.vd_pdbqt_ligand(text.encode(), C.byref(h), C.byref(d))
+            if st == 0:
+                assert d.n_atoms > 0 and d.n_nodes > 0
+                pose = (C.c_float * (7 + vdock.MAX_TORS))(*([0.0] * (7 + vdock.MAX_TORS)))
+                pose[3] = 1.0
+                xyz = (C.c_double * (3 * d.n_atoms))()
+                assert lib.vd_conf_to_coords(C.byref(d), pose, xyz) == 0
+                n = C.c_int64()
+                assert lib.vd_pdbqt_write_model(h, xyz, None, 0, C.byref(n)) == 0
+                buf = C.create_string_buffer(n.value + 1)
+                assert lib.vd_pdbqt_write_model(h, xyz, buf, n.value + 1, C.byref(n)) == 0
+                lib.vd_pdbqt_free(h)
+        else:
+            text = "\n".join(_mutate(rec, rng))
+            h, n = C.c_void_p(), C.c_int32()
+            x, s = C.POINTER(C.c_double)(), C.POINTER(C.c_int32)()
+            st = lib.vd_pdbqt_receptor(text.encode(), C.byref(h), C.byref(n), C.byref(x), C.byref(s))
+            if st == 0:
+                lib.vd_pdbqt_free(h)
+        assert st in (0, 5), st
+        seen[st] += 1
+    assert seen[0] > 100 and seen[5] > 100
