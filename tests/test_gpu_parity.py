@@ -258,3 +258,46 @@ def test_docking_pipeline_matches_oracle_pipeline(vd):
     # the returned score of mode 1 is the score of the returned pose
     p0 = r["pose"][0].astype(np.float64)
     assert abs(orc.eval_adjusted(lo, p0, orc.intramolecular(lo, p0)) - e[0]) <= 2e-3
+
+
+def test_pipeline_score_and_pose_distributions_over_seeds(vd):
+    """Best final score and top pose of the plain docking pipeline over 8
+    seeds, GPU against the oracle's restatement of the same pipeline (the
+    two take different FP paths, so runs are compared as distributions):
+    paired best scores within 0.6 kcal/mol in median and medians within
+    0.3 kcal/mol; the top poses' heavy-atom RMSD to the best pose found by
+    either (the run-to-run spread of the search) has the same distribution:
+    two-sample KS p >= 0.01, and the counts of runs that found the best
+    site (within 2 A) agree by Fisher's exact test (p >= 0.01) -- the RMSDs
+    are bimodal (the best site, or another site ~10 A away in this box), so
+    medians of 8 runs are not a usable statistic."""
+    from scipy.stats import fisher_exact, ks_2samp
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=20, n_tors=4, seed=31, box=20.0, radius=40.0)
+    gpu, ref = [], []
+    for seed in range(1, 9):
+        sp = vd.search_params(seed=seed, n_chains=512, search_depth=6, max_bfgs_steps=15, num_modes=9)
+        r = ctx.dock_plain(lc, sp)
+        gpu.append((float(r["energy"][0]), r["pose"][0].astype(np.float64)))
+        conf, ec, _ = orc.mc_chains(lo, seed, lc, 6, 15, 0, 512, threads=8)
+        refined = []
+        for i in orc.cluster(lo, conf, ec, 1.0, 20):
+            er, c, _ = orc.refine(lo, conf[i], 15)
+            if er < 1e30:
+                refined.append((er, c))
+        refined.sort(key=lambda t: t[0])
+        ib = orc.intramolecular(lo, refined[0][1])
+        scored = sorted(((orc.eval_adjusted(lo, c, ib), c) for _, c in refined), key=lambda t: t[0])
+        ref.append(scored[0])
+    eg = np.array([g[0] for g in gpu])
+    er = np.array([r[0] for r in ref])
+    assert np.median(np.abs(eg - er)) <= 0.6, (eg, er)
+    assert abs(np.median(eg) - np.median(er)) <= 0.3, (eg, er)
+    na = lig["n_atoms"]
+    allp = [g[1] for g in gpu] + [r[1] for r in ref]
+    best = allp[int(np.argmin(np.concatenate([eg, er])))]
+    xb = orc.coords(lo, best, na).ravel()
+    rg = np.array([orc.rmsd(lo, orc.coords(lo, p, na).ravel(), xb)[1] for p in allp[:8]])
+    rr = np.array([orc.rmsd(lo, orc.coords(lo, p, na).ravel(), xb)[1] for p in allp[8:]])
+    assert ks_2samp(rg, rr).pvalue >= 0.01, (rg, rr)
+    hit_g, hit_r = int((rg < 2.0).sum()), int((rr < 2.0).sum())
+    assert fisher_exact([[hit_g, 8 - hit_g], [hit_r, 8 - hit_r]])[1] >= 0.01, (rg, rr)
