@@ -50,6 +50,8 @@ def args_():
     a.add_argument("--cpu-ligands", type=int, default=3, help="whole ligands in the CPU sample")
     a.add_argument("--no-configs", action="store_true", help="skip the plain / adjoint / uneven-batch lines")
     a.add_argument("--launch-shape", type=int, default=0, help="docking kernel shape (0 = autotuned, 1-3 pinned)")
+    a.add_argument("--configs", default="plain,adjoint,uneven", help="secondary lines to run (comma list)")
+    a.add_argument("--only-configs", action="store_true", help="skip the headline; print the secondary lines")
     return a.parse_args()
 
 
@@ -171,7 +173,7 @@ def cpu_baseline(xyz, xs, ligs, chains_per_lig, n_sample):
             "grid_build_s": t_grid, "bfgs_evals_per_s": total_evals / total_t}
 
 
-def secondary_configs(hbm, cpu):
+def secondary_configs(hbm, cpu, which=("plain", "adjoint", "uneven")):
     """The reference's other named workloads, measured once each on one GPU
     (synthetic inputs of the named shapes; seeded):
       plain_single_ligand : 24-atom / 5-torsion ligand, 2,000-atom receptor,
@@ -185,19 +187,26 @@ def secondary_configs(hbm, cpu):
                             atom receptor, 30 A box, 8,192 chains (16 per
                             ligand) x 2,000 MC steps in one batched call.
     Each carries the oracle port timed on a bounded sample on the host cores."""
-    import numpy as np
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    threads = os.cpu_count() or 1
+    out = {}
+    if "plain" in which:
+        out["plain_single_ligand"] = _plain_line(hbm, cpu, threads)
+    if "adjoint" in which:
+        out["adjoint_poses"] = _adjoint_line(hbm, cpu)
+    if "uneven" in which:
+        out["batched_uneven"] = _uneven_line(cpu, threads)
+    return out
+
+
+def _plain_line(hbm, cpu, threads):
     import torch
     import vdock
     from vdock import synth
-    sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle_lib
-    threads = os.cpu_count() or 1
-    out = {}
 
     def lig_cost_bytes(lig):
         return 32 * int((lig["xs"] >= 0).sum()) + 16 * len(lig["pairs"])
-
-    # -- plain single ligand (1,024 chains x 1,000 steps)
     cfg = synth.CONFIGS["plain"]
     xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED + 1)
     lig = synth.ligand(cfg["lig_atoms"], cfg["lig_tors"], SEED + 2)
@@ -233,9 +242,18 @@ def secondary_configs(hbm, cpu):
                                 "cores": threads, "kind": "port",
                                 "sample": f"{n_s} of {cfg['chains']} chains x {cfg['steps']} steps, "
                                           f"extrapolated to all chains (MC search only)"}
-    out["plain_single_ligand"] = line
+    return line
 
-    # -- adjoint: 65,536 poses, energy + gradient and energy only
+
+def _adjoint_line(hbm, cpu):
+    import numpy as np
+    import torch
+    import vdock
+    from vdock import synth
+    import oracle_lib
+
+    def lig_cost_bytes(lig):
+        return 32 * int((lig["xs"] >= 0).sum()) + 16 * len(lig["pairs"])
     cfg = synth.CONFIGS["adjoint"]
     xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED + 1)
     lig = synth.ligand(cfg["lig_atoms"], cfg["lig_tors"], SEED + 3)
@@ -281,9 +299,14 @@ def secondary_configs(hbm, cpu):
         dt = time.perf_counter() - t0
         line["cpu_baseline"] = {"evals_per_s": n_s / dt, "cores": 1, "kind": "port",
                                 "sample": f"{n_s} of {n} poses, energy + gradient, one thread"}
-    out["adjoint_poses"] = line
+    return line
 
-    # -- batched uneven: 512 ligands, 8,192 chains x 2,000 steps
+
+def _uneven_line(cpu, threads):
+    import torch
+    import vdock
+    from vdock import synth
+    import oracle_lib
     cfg = synth.CONFIGS["batched"]
     xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED + 5)
     ligs = synth.ligand_set(cfg["ligands"], cfg["atoms"], cfg["tors"], SEED + 6)
@@ -320,8 +343,7 @@ def secondary_configs(hbm, cpu):
         line["cpu_baseline"] = {"bfgs_evals_per_s": cev / dt, "cores": threads, "kind": "port",
                                 "sample": f"{n_s} of {len(ids)} ligands, {per} chains x {cfg['steps']} steps "
                                           f"(MC search only)"}
-    out["batched_uneven"] = line
-    return out
+    return line
 
 
 def run_reference(a):
@@ -465,12 +487,18 @@ def run_ours(a):
         line["grid_build"]["cpu_s"] = cb["grid_build_s"]
     ctx.close()
     if world == 1 and not a.no_configs:
-        line["configs"] = secondary_configs(hbm, not a.no_cpu_baseline)
+        line["configs"] = secondary_configs(hbm, not a.no_cpu_baseline, a.configs.split(","))
     print(json.dumps(line), flush=True)
 
 
 def main():
     a = args_()
+    if a.only_configs:
+        import torch
+        torch.cuda.set_device(0)
+        hbm, _ = peaks()
+        print(json.dumps({"configs": secondary_configs(hbm, not a.no_cpu_baseline, a.configs.split(","))}), flush=True)
+        return
     if a.impl == "reference":
         run_reference(a)
     else:

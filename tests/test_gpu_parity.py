@@ -301,3 +301,38 @@ def test_pipeline_score_and_pose_distributions_over_seeds(vd):
     assert ks_2samp(rg, rr).pvalue >= 0.01, (rg, rr)
     hit_g, hit_r = int((rg < 2.0).sum()), int((rr < 2.0).sum())
     assert fisher_exact([[hit_g, 8 - hit_g], [hit_r, 8 - hit_r]])[1] >= 0.01, (rg, rr)
+
+
+def test_abi_rejects_malformed_inputs(vd):
+    """Inputs that could otherwise reach a kernel malformed are rejected on the
+    host with VD_ERR_ARG (3) or VD_ERR_CAPACITY (2), and the context stays usable."""
+    import ctypes as C
+    from vdock import synth
+    ctx = vd.Context()
+    L = ctx.L
+    c3 = C.c_double * 3
+    for center, size, want in (((0, 0, 0), (float("inf"), 10, 10), 3), ((float("nan"), 0, 0), (10, 10, 10), 3),
+                               ((0, 0, 0), (1e12, 10, 10), 2), ((0, 0, 0), (-1, 10, 10), 3),
+                               ((0, 0, 0), (2000, 2000, 2000), 2)):
+        assert L.vd_set_box(ctx.h, c3(*center), c3(*size)) == want, (center, size)
+    xyz, xs = synth.receptor(300, 15.0, 2)
+    bad = xyz.copy()
+    bad[7, 1] = float("nan")
+    with pytest.raises(RuntimeError):
+        ctx.set_receptor(bad, xs)
+    lig = synth.ligand(15, 2, 3)
+    badl = dict(lig)
+    badl["xyz"] = lig["xyz"].copy()
+    badl["xyz"][2, 0] = float("inf")
+    with pytest.raises(RuntimeError):
+        ctx.add_ligand(badl)
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0, 0, 0], [10, 10, 10])
+    ctx.build_grids(synth.TYPES8)
+    lid = ctx.add_ligand(lig)
+    with pytest.raises(RuntimeError):  # 2^31 work items would overflow the item counter
+        ctx.dock_batched([lid] * 3, vd.search_params(n_chains=1 << 29))
+    with pytest.raises(RuntimeError):
+        ctx.energy(lid + 5, synth.random_poses(4, ctx.ntors[lid], -2, 2, 1))
+    e, g = ctx.energy_grad(lid, synth.random_poses(8, ctx.ntors[lid], -2, 2, 1))  # still usable
+    assert np.all(np.isfinite(e)) and np.all(np.isfinite(g))

@@ -168,8 +168,12 @@ vd_status vd_get_tables(vd_ctx* h, double* fast, double* se, double* sd) {
 vd_status vd_set_receptor(vd_ctx* h, int32_t n, const double* xyz, const int32_t* xs) {
     VD_CHECK(h && n >= 0 && (n == 0 || (xyz && xs)), VD_ERR_ARG, "vd_set_receptor: bad arguments");
     Ctx& c = h->c;
-    for (int i = 0; i < n; ++i)
+    for (int i = 0; i < n; ++i) {
         VD_CHECK(xs[i] >= -1 && xs[i] < kTypes, VD_ERR_ARG, "vd_set_receptor: XS type out of range");
+        VD_CHECK(std::isfinite(xyz[3 * size_t(i)]) && std::isfinite(xyz[3 * size_t(i) + 1]) &&
+                     std::isfinite(xyz[3 * size_t(i) + 2]),
+                 VD_ERR_ARG, "vd_set_receptor: non-finite coordinate");
+    }
     c.rec_xyz.assign(xyz, xyz + 3 * size_t(n));
     c.rec_xs.assign(xs, xs + n);
     c.n_maps = 0;
@@ -184,6 +188,9 @@ vd_status vd_set_box(vd_ctx* h, const double center[3], const double size[3]) {
     GridGeom& g = c.geom;
     for (int i = 0; i < 3; ++i) {
         VD_CHECK(size[i] > 0, VD_ERR_ARG, "vd_set_box: search space dimensions must be positive");
+        VD_CHECK(std::isfinite(center[i]) && std::isfinite(size[i]), VD_ERR_ARG,
+                 "vd_set_box: center and size must be finite");
+        VD_CHECK(size[i] <= 1e5, VD_ERR_CAPACITY, "vd_set_box: box too large for one map (2^31 points)");
         const double granularity = 0.375;
         const int n = int(std::ceil(size[i] / granularity));
         const double real_span = granularity * n;

@@ -169,6 +169,8 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
                        DockBuffers& out) {
     VD_CHECK(!ligs.empty(), VD_ERR_ARG, "no ligands");
     VD_CHECK(sp.n_chains > 0, VD_ERR_ARG, "n_chains must be positive");
+    VD_CHECK(int64_t(ligs.size()) * sp.n_chains <= (int64_t(1) << 30), VD_ERR_CAPACITY,
+             "more than 2^30 (ligand, chain) work items in one call");
     VD_CHECK(c.has_box, VD_ERR_ARG, "no box set");
     vd_status st = sync_pool(&c);
     if (st != VD_OK) return st;

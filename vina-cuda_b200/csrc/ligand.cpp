@@ -105,6 +105,9 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     for (int i = 0; i < na; ++i) {
         VD_CHECK(d->xs[i] >= -1 && d->xs[i] < kTypes, VD_ERR_ARG, "vd_add_ligand: XS type out of range");
         VD_CHECK(d->atom_node[i] >= 0 && d->atom_node[i] < nn, VD_ERR_ARG, "vd_add_ligand: atom_node out of range");
+        VD_CHECK(std::isfinite(d->xyz[3 * size_t(i)]) && std::isfinite(d->xyz[3 * size_t(i) + 1]) &&
+                     std::isfinite(d->xyz[3 * size_t(i) + 2]),
+                 VD_ERR_ARG, "vd_add_ligand: non-finite coordinate");
         VD_CHECK(i == 0 || d->atom_node[i] >= d->atom_node[i - 1], VD_ERR_ARG,
                  "vd_add_ligand: atoms must be grouped by rigid body in body order");
         if (d->xs[i] >= 0) {
