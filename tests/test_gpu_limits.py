@@ -69,3 +69,45 @@ def test_ligands_beyond_the_limits_are_rejected(env, na, nt, seed):
     lig = synth.ligand(na, nt, seed)
     with pytest.raises(RuntimeError, match="error 2"):
         ctx.add_ligand(lig)
+
+
+def test_empty_receptor_and_empty_box(env):
+    """No receptor atoms at all, and a box far from every receptor atom: the
+    maps are zero, energies are the intramolecular term (plus the out-of-box
+    penalty) as in the oracle -- 1e-3 kcal/mol for poses inside the box; a
+    pose partly outside carries slope 1e6 kcal/mol/A times the FP32
+    coordinate rounding (~1e-6 A), so 1e-4 relative + 1 kcal/mol per atom
+    outside -- and plain and batched docking still return valid modes."""
+    vd, _, _ = env
+    from vdock import synth
+    lig = synth.ligand(20, 4, 8)
+    for xyz, xs, center in ((np.zeros((0, 3)), np.zeros(0, dtype=np.int32), (0.0, 0.0, 0.0)),
+                            (*synth.receptor(300, 20.0, 3), (200.0, 0.0, 0.0))):
+        ctx = vd.Context()
+        orc = O.Oracle()
+        for o in (ctx, orc):
+            o.set_receptor(xyz, xs)
+            o.set_box(list(center), [24.0] * 3)
+        types = sorted(set(int(t) for t in lig["xs"] if t >= 0))
+        ctx.build_grids(types)
+        orc.build_grids(types)
+        for t in types:
+            assert not np.any(ctx.grid(t))
+        lc, lo = ctx.add_ligand(lig), orc.add_ligand(lig)
+        poses = synth.random_poses(16, ctx.ntors[lc], -3.0, 3.0, seed=4)
+        poses[:, :3] += np.asarray(center, dtype=np.float32)
+        e, g = ctx.energy_grad(lc, poses)
+        _, bmin, bmax = orc.grid_info()
+        inside = 0
+        for i, p in enumerate(poses):
+            e_ref, g_ref = orc.eval_deriv(lo, p.astype(np.float64))
+            x = orc.coords(lo, p.astype(np.float64), lig["n_atoms"])
+            out = int(np.sum(np.any((x < bmin) | (x > bmax), axis=1)))
+            inside += out == 0
+            assert abs(e[i] - e_ref) <= (1e-3 if out == 0 else 1e-4 * abs(e_ref) + 1.0 * out), (i, e[i], e_ref, out)
+        assert inside >= 8
+        sp = vd.search_params(seed=2, n_chains=128, search_depth=2, max_bfgs_steps=10)
+        r = ctx.dock_plain(lc, sp)
+        rb = ctx.dock_batched([lc, ctx.add_ligand(synth.ligand(14, 2, 9))], sp)
+        for res in [r] + rb:
+            assert 1 <= len(res["energy"]) and np.all(np.isfinite(res["energy"]))
