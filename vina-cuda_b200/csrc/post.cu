@@ -10,6 +10,9 @@
 //   score   : eval_intramolecular of the best mode and eval_adjusted
 //             (model.cpp:1375-1431) in double, remove_redundant, the
 //             num_modes / energy_range cut and RMSD bounds to mode 1
+// dock_pipeline runs the docking launch and these kernels; the batched form
+// records the whole sequence, with its uploads and downloads, into one CUDA
+// graph per call (updated in place for the next call of the same shape).
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
