@@ -35,7 +35,9 @@ typedef enum {
     VD_ERR_CUDA = 1,      /* a CUDA runtime call failed                        */
     VD_ERR_CAPACITY = 2,  /* input exceeds a compiled limit (atoms, torsions)  */
     VD_ERR_ARG = 3,       /* invalid argument or call order                    */
-    VD_ERR_TIMEOUT = 4,   /* a device loop hit its iteration budget            */
+    VD_ERR_TIMEOUT = 4,   /* reserved: every device loop here is bounded by its
+                             inputs and no kernel waits on another, so no call
+                             returns it today                                 */
     VD_ERR_PARSE = 5,     /* malformed PDBQT / config input                    */
     VD_ERR_NOMEM = 6      /* allocation failed or the context memory cap hit   */
 } vd_status;
