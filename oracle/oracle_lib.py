@@ -45,6 +45,10 @@ def lib():
         L.or_get_grid.argtypes = [vp, C.c_int, dp]
         L.or_add_ligand.argtypes = [vp, vp]
         L.or_ligand_ntors.argtypes = [vp, C.c_int]
+        L.or_term_values_coords.restype = None
+        L.or_term_values_coords.argtypes = [vp, C.c_int, dp, dp]
+        L.or_conf_independent.restype = C.c_double
+        L.or_conf_independent.argtypes = [vp, C.c_int, C.c_double]
         L.or_maps_ready.restype = C.c_int
         L.or_maps_ready.argtypes = [vp, C.c_int]
         L.or_eval_deriv.restype = C.c_double
@@ -215,6 +219,16 @@ class Oracle:
     def eval_adjusted_coords(self, lig, xyz, intra_best):
         x, xp = _d(xyz)
         return self.L.or_eval_adjusted_coords(self.h, lig, xp, intra_best)
+
+    def term_values(self, lig, xyz):
+        """Unweighted intermolecular terms of heavy-atom coordinates (--score_only breakdown)."""
+        x, xp = _d(np.asarray(xyz, dtype=np.float64).ravel())
+        out, op = _d(np.zeros(5))
+        self.L.or_term_values_coords(self.h, lig, xp, op)
+        return out.copy()
+
+    def conf_independent(self, lig, x):
+        return self.L.or_conf_independent(self.h, lig, float(x))
 
     def rmsd(self, lig, a, b):
         a, ap = _d(a)

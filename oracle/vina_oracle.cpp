@@ -1096,6 +1096,28 @@ double or_eval_adjusted_coords(or_ctx* c, int lig, const double* xyz, double int
     double e = nc_eval_coords(c, L, v, 1000.0, 1e6) + intra_fast_coords(c, L, v, 1000.0);
     return conf_independent(c, L, e - intra_best);
 }
+// terms.cpp:385-446 (evale_robust): the five unweighted intermolecular
+// terms, evaluated analytically at each ligand-receptor heavy-atom distance
+// up to the 8 A cutoff (what --score_only prints, main.cpp:191-218).
+void or_term_values_coords(or_ctx* c, int lig, const double* xyz, double out[5]) {
+    const Lig& L = c->ligs[lig];
+    const std::vector<V3> v = to_v3(xyz, L.na);
+    for (int k = 0; k < 5; ++k) out[k] = 0;
+    for (int i = 0; i < L.na; ++i) {
+        if (L.xs[i] < 0 || L.xs[i] >= kTypes) continue;
+        for (size_t j = 0; j < c->rec_xyz.size(); ++j) {
+            const int t2 = c->rec_xs[j];
+            if (t2 < 0 || t2 >= kTypes) continue;
+            const double d2 = dist_sqr(v[i], c->rec_xyz[j]);
+            if (d2 > kCutoff * kCutoff) continue;
+            double t[5];
+            raw_terms(L.xs[i], t2, std::sqrt(d2), t);
+            for (int k = 0; k < 5; ++k) out[k] += t[k];
+        }
+    }
+}
+double or_conf_independent(or_ctx* c, int lig, double x) { return conf_independent(c, c->ligs[lig], x); }
+
 double or_eval_adjusted(or_ctx* c, int lig, const double* conf, double intra_best) {
     Frames F;
     const Lig& L = c->ligs[lig];

@@ -58,6 +58,11 @@ int     or_maps_ready(or_ctx*, int lig);
 /* conf layout: pos[3], quat[4] (w,x,y,z), torsions[ntors]
  * grad layout: force[3], torque[3], torsion grads[ntors]
  * v[3] = (intra cap, inter cap, other-pair cap) as in model.cpp:1324. */
+/* Unweighted intermolecular terms (gauss1, gauss2, repulsion, hydrophobic,
+ * hydrogen bond) of heavy-atom coordinates xyz, analytic (terms.cpp:385-446),
+ * and the torsion normalisation x / (1 + w N_tors / 5) (everything.cpp:294-301). */
+void    or_term_values_coords(or_ctx*, int lig, const double* xyz, double out[5]);
+double  or_conf_independent(or_ctx*, int lig, double x);
 double  or_eval_deriv(or_ctx*, int lig, const double* conf, const double v[3],
                       double slope, double* grad /* may be NULL */);
 void    or_coords(or_ctx*, int lig, const double* conf, double* xyz_out /* all atoms */);

@@ -187,3 +187,33 @@ def test_oracle_refuses_unbuilt_maps():
     o.build_grids(sorted(set(int(t) for t in lig["xs"] if t >= 0)))
     assert o.L.or_maps_ready(o.h, lid) == 1
     assert np.isfinite(o.eval_deriv(lid, conf)[0])
+
+
+def test_score_only_term_breakdown_is_consistent(golden_dir):
+    """The --score_only self-check of the reference (main.cpp:191-218): the
+    five unweighted intermolecular terms evaluated analytically at the exact
+    distances (terms.cpp:385-446), weighted and divided by the torsion
+    normalisation, agree with the table-based affinity of the same pose to
+    0.05 kcal/mol whenever that affinity is below 100.  Run over every mode
+    of the reference's docked outputs, this checks the interpolated pair
+    tables against the analytic terms they sample."""
+    z = load(golden_dir)
+    w = O.DEFAULT_WEIGHTS
+    worst, n = 0.0, 0
+    for i, name in enumerate(z["names"]):
+        o = O.Oracle()
+        o.set_receptor(z["rec_xyz"], z["rec_xs"])
+        o.set_box(z["center"], z["size"])
+        d, models, _ = ligand(z, f"L{i}")
+        lid = o.add_ligand(d)
+        for m in models:
+            e = o.eval_adjusted_coords(lid, m, o.intramolecular_coords(lid, m))
+            terms = o.term_values(lid, m)
+            assert terms.shape == (5,) and np.all(np.isfinite(terms))
+            e2 = o.conf_independent(lid, float(np.dot(terms, w[:5])))
+            if e < 100:
+                worst = max(worst, abs(e2 - e))
+                n += 1
+                assert abs(e2 - e) <= 0.05, (name, e, e2, terms)
+    assert n >= 300
+    print(f"score_only breakdown: {n} poses, worst |sum w*term - affinity| = {worst:.4f}")
