@@ -39,7 +39,8 @@ typedef enum {
                              inputs and no kernel waits on another, so no call
                              returns it today                                 */
     VD_ERR_PARSE = 5,     /* malformed PDBQT / config input                    */
-    VD_ERR_NOMEM = 6      /* allocation failed or the context memory cap hit   */
+    VD_ERR_NOMEM = 6      /* device out of memory or the context's cap hit
+                             (vd_set_memory_cap); the context stays usable     */
 } vd_status;
 
 #define VD_MAX_ATOMS 128      /* heavy atoms per ligand (inc/kernel2.h:36)      */
@@ -117,6 +118,8 @@ typedef struct {
     int64_t graph_launches;      /* batched pipelines submitted as a CUDA graph */
     int64_t graph_instantiations;/* executables built (the rest were updated in place) */
     double  scoring_ms;          /* wall time of the last vd_set_scoring(_device) */
+    int64_t device_bytes;        /* device memory the context holds for maps, tables,
+                                    ligands, receptor cells and scratch           */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -124,6 +127,12 @@ vd_status vd_create(vd_ctx** out, int device);
 vd_status vd_destroy(vd_ctx* ctx);
 const char* vd_last_error(void);
 vd_status vd_get_stats(vd_ctx* ctx, vd_stats* out);
+/* Caps the device memory the context may hold (bytes; 0 = no cap, the
+ * default).  A call that would allocate past it -- or that finds the device
+ * out of memory -- fails with VD_ERR_NOMEM and leaves the context usable:
+ * raise the cap (or free work) and call again.  No reference counterpart
+ * (the reference sizes its buffers statically, kernel2.h:46-52). */
+vd_status vd_set_memory_cap(vd_ctx* ctx, int64_t bytes);
 
 /* ---- scoring, receptor, box (main.cpp:337-345, 856-876) ------------------ */
 /* weights: gauss1, gauss2, repulsion, hydrophobic, hydrogen, and the internal

@@ -1,4 +1,5 @@
 // Context lifetime, errors, scoring tables, receptor and box set-up.
+#include <algorithm>
 #include <cmath>
 #include <chrono>
 #include <cstring>
@@ -12,13 +13,49 @@ namespace vd {
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
 
+vd_status dev_alloc(Ctx& c, void** p, size_t bytes, const char* what) {
+    *p = nullptr;
+    if (c.dev_cap > 0 && c.dev_used + bytes > c.dev_cap) {
+        set_error(std::string(what) + ": " + std::to_string(bytes) + " bytes would exceed the context's device memory cap (" +
+                  std::to_string(c.dev_used) + " of " + std::to_string(c.dev_cap) + " in use)");
+        return VD_ERR_NOMEM;
+    }
+    const cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 1));
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();  // not sticky: clear it so the context stays usable
+        *p = nullptr;
+        set_error(std::string(what) + ": out of device memory for " + std::to_string(bytes) + " bytes");
+        return VD_ERR_NOMEM;
+    }
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        set_error(std::string(what) + ": cudaMalloc: " + cudaGetErrorString(e));
+        return VD_ERR_CUDA;
+    }
+    c.dev_bytes[*p] = bytes;
+    c.dev_used += bytes;
+    return VD_OK;
+}
+
+void dev_free(Ctx& c, void* p) {
+    if (!p) return;
+    auto it = c.dev_bytes.find(p);
+    if (it != c.dev_bytes.end()) {
+        c.dev_used -= it->second;
+        c.dev_bytes.erase(it);
+    }
+    cudaFree(p);
+}
+
 vd_status ensure_scratch(Ctx* c, size_t bytes) {
     if (c->scratch_bytes >= bytes) return VD_OK;
-    if (c->d_scratch) VD_CUDA(cudaFree(c->d_scratch));
-    c->d_scratch = nullptr;
+    dev_release(*c, c->d_scratch);
     c->scratch_bytes = 0;
     size_t want = bytes + bytes / 4;
-    VD_CUDA(cudaMalloc(&c->d_scratch, want));
+    if (c->dev_cap > 0 && c->dev_used + want > c->dev_cap && c->dev_used + bytes <= c->dev_cap)
+        want = bytes;  // under a cap, give up the growth headroom before failing
+    vd_status st = dev_alloc(*c, &c->d_scratch, want, "scratch");
+    if (st != VD_OK) return st;
     c->scratch_bytes = want;
     return VD_OK;
 }
@@ -101,8 +138,15 @@ vd_status vd_destroy(vd_ctx* h) {
     return VD_OK;
 }
 
+vd_status vd_set_memory_cap(vd_ctx* h, int64_t bytes) {
+    VD_CHECK(h && bytes >= 0, VD_ERR_ARG, "vd_set_memory_cap: bad arguments");
+    h->c.dev_cap = size_t(bytes);
+    return VD_OK;
+}
+
 vd_status vd_get_stats(vd_ctx* h, vd_stats* out) {
     VD_CHECK(h && out, VD_ERR_ARG, "vd_get_stats: NULL argument");
+    h->c.stats.device_bytes = int64_t(h->c.dev_used);
     *out = h->c.stats;
     return VD_OK;
 }
@@ -131,12 +175,15 @@ vd_status vd_set_scoring(vd_ctx* h, const double weights[6]) {
             s[size_t(p) * kBins + i] = make_float4(float(c.se[b + i]), float(c.sd[b + i]),
                                                    float(c.se[b + i + 1]), float(c.sd[b + i + 1]));
         }
-    if (!c.d_fast) VD_CUDA(cudaMalloc(&c.d_fast, f.size() * sizeof(float)));
-    if (!c.d_smooth) VD_CUDA(cudaMalloc(&c.d_smooth, s.size() * sizeof(float4)));
+    vd_status st = VD_OK;
+    if (!c.d_fast && (st = dev_alloc(c, &c.d_fast, f.size() * sizeof(float), "pair tables")) != VD_OK) return st;
+    if (!c.d_smooth && (st = dev_alloc(c, &c.d_smooth, s.size() * sizeof(float4), "pair tables")) != VD_OK)
+        return st;
     std::vector<double> fd(size_t(kPairTypes) * kBins);
     for (int p = 0; p < kPairTypes; ++p)
         for (int i = 0; i < kBins; ++i) fd[size_t(p) * kBins + i] = c.fast[size_t(p) * kN + i];
-    if (!c.d_fastd) VD_CUDA(cudaMalloc(&c.d_fastd, fd.size() * sizeof(double)));
+    if (!c.d_fastd && (st = dev_alloc(c, &c.d_fastd, fd.size() * sizeof(double), "pair tables")) != VD_OK)
+        return st;
     VD_CUDA(cudaMemcpy(c.d_fastd, fd.data(), fd.size() * sizeof(double), cudaMemcpyHostToDevice));
     VD_CUDA(cudaMemcpy(c.d_fast, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
     VD_CUDA(cudaMemcpy(c.d_smooth, s.data(), s.size() * sizeof(float4), cudaMemcpyHostToDevice));

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -145,6 +146,11 @@ struct Ctx {
     size_t h_stage_bytes = 0;
     cudaGraphExec_t pipe_exec = nullptr;
     vd_stats stats{};
+    // device memory owned by the context (dev_alloc / dev_free): bytes in use
+    // per allocation, and an optional cap (0 = none) that turns an allocation
+    // past it into VD_ERR_NOMEM
+    std::unordered_map<void*, size_t> dev_bytes;
+    size_t dev_used = 0, dev_cap = 0;
     // launch-shape autotuners (tune.h); grid_shape_fixed > 0 pins the grid tile
     Tuner dock_tune, grid_tune;
     int grid_shape_fixed = 0;
@@ -161,6 +167,23 @@ inline cudaError_t record_event(cudaEvent_t e, cudaStream_t s) {
 }
 
 vd_status ensure_scratch(Ctx* c, size_t bytes);
+// Context-owned device allocation: VD_ERR_NOMEM past the context's cap or
+// when the device is out of memory; *p is null on failure.
+vd_status dev_alloc(Ctx& c, void** p, size_t bytes, const char* what);
+template <class T>
+vd_status dev_alloc(Ctx& c, T** p, size_t bytes, const char* what) {
+    void* q = nullptr;
+    const vd_status st = dev_alloc(c, &q, bytes, what);
+    *p = static_cast<T*>(q);
+    return st;
+}
+// Frees a dev_alloc allocation (null is fine) and sets the pointer to null.
+void dev_free(Ctx& c, void* p);
+template <class T>
+void dev_release(Ctx& c, T*& p) {
+    dev_free(c, p);
+    p = nullptr;
+}
 vd_status ensure_host_stage(Ctx* c, size_t bytes);
 vd_status sync_pool(Ctx* c);
 vd_status ensure_receptor_cells(Ctx* c);

@@ -355,9 +355,11 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
     const size_t bytes_atoms = std::max<size_t>(1, sorted.size()) * sizeof(StagedAtom);
     const size_t bytes_start = start.size() * sizeof(int32_t);
     const size_t bytes_lut = lut.size() * sizeof(float);
-    if (c.d_maps) VD_CUDA(cudaFree(c.d_maps));
-    c.d_maps = nullptr;
-    VD_CUDA(cudaMalloc(&c.d_maps, bytes_maps));
+    dev_release(c, c.d_maps);
+    c.n_maps = 0;
+    for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
+    vd_status st0 = dev_alloc(c, &c.d_maps, bytes_maps, "vd_build_grids: maps");
+    if (st0 != VD_OK) return st0;
     vd_status st = ensure_scratch(&c, bytes_atoms + bytes_start + bytes_lut + 256);
     if (st != VD_OK) return st;
     char* s = static_cast<char*>(c.d_scratch);

@@ -17,7 +17,8 @@ vd_status sync_pool(Ctx* c) {
     if (words > c->pool_cap || !c->d_pool) {
         const int64_t cap = std::max<int64_t>(words + words / 2, 4096);
         float4* fresh = nullptr;
-        VD_CUDA(cudaMalloc(&fresh, size_t(cap) * sizeof(float4)));
+        vd_status st = dev_alloc(*c, &fresh, size_t(cap) * sizeof(float4), "ligand pool");
+        if (st != VD_OK) return st;
         int64_t keep = 0;
         if (c->pool_synced > 0) {
             const HostLigand& last = c->ligs[c->pool_synced - 1];
@@ -27,7 +28,7 @@ vd_status sync_pool(Ctx* c) {
             VD_CUDA(cudaMemcpyAsync(fresh, c->d_pool, size_t(keep) * sizeof(float4), cudaMemcpyDeviceToDevice,
                                     c->stream));
         VD_CUDA(cudaStreamSynchronize(c->stream));
-        if (c->d_pool) VD_CUDA(cudaFree(c->d_pool));
+        dev_release(*c, c->d_pool);
         c->d_pool = fresh;
         c->pool_cap = cap;
     }

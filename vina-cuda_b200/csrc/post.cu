@@ -658,12 +658,22 @@ vd_status ensure_receptor_cells(Ctx* c) {
         rf[r] = make_float4(float(a[0]), float(a[1]), float(a[2]), float(c->rec_xs[rel[r]]));
         rd[r] = make_double4(a[0], a[1], a[2], double(c->rec_xs[rel[r]]));
     }
-    cudaFree(c->d_rec); cudaFree(c->d_recd); cudaFree(c->d_cell_start); cudaFree(c->d_cell_list);
-    c->d_rec = nullptr; c->d_recd = nullptr; c->d_cell_start = nullptr; c->d_cell_list = nullptr;
-    VD_CUDA(cudaMalloc(&c->d_rec, rf.size() * sizeof(float4)));
-    VD_CUDA(cudaMalloc(&c->d_recd, rd.size() * sizeof(double4)));
-    VD_CUDA(cudaMalloc(&c->d_cell_start, start.size() * sizeof(int32_t)));
-    VD_CUDA(cudaMalloc(&c->d_cell_list, std::max<size_t>(1, list.size()) * sizeof(int32_t)));
+    dev_release(*c, c->d_rec);
+    dev_release(*c, c->d_recd);
+    dev_release(*c, c->d_cell_start);
+    dev_release(*c, c->d_cell_list);
+    vd_status st = dev_alloc(*c, &c->d_rec, rf.size() * sizeof(float4), "receptor cells");
+    if (st == VD_OK) st = dev_alloc(*c, &c->d_recd, rd.size() * sizeof(double4), "receptor cells");
+    if (st == VD_OK) st = dev_alloc(*c, &c->d_cell_start, start.size() * sizeof(int32_t), "receptor cells");
+    if (st == VD_OK)
+        st = dev_alloc(*c, &c->d_cell_list, std::max<size_t>(1, list.size()) * sizeof(int32_t), "receptor cells");
+    if (st != VD_OK) {
+        dev_release(*c, c->d_rec);
+        dev_release(*c, c->d_recd);
+        dev_release(*c, c->d_cell_start);
+        dev_release(*c, c->d_cell_list);
+        return st;
+    }
     VD_CUDA(cudaMemcpy(c->d_rec, rf.data(), rf.size() * sizeof(float4), cudaMemcpyHostToDevice));
     VD_CUDA(cudaMemcpy(c->d_recd, rd.data(), rd.size() * sizeof(double4), cudaMemcpyHostToDevice));
     VD_CUDA(cudaMemcpy(c->d_cell_start, start.data(), start.size() * sizeof(int32_t), cudaMemcpyHostToDevice));

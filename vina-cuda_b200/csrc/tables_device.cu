@@ -63,10 +63,11 @@ __global__ void __launch_bounds__(256) tables_kernel(TableParams p) {
 
 vd_status build_tables_device(Ctx& c, const double w[6]) {
     const size_t n = size_t(kPairTypes) * kN, nb = size_t(kPairTypes) * kBins;
-    if (!c.d_fast) VD_CUDA(cudaMalloc(&c.d_fast, nb * sizeof(float)));
-    if (!c.d_smooth) VD_CUDA(cudaMalloc(&c.d_smooth, nb * sizeof(float4)));
-    if (!c.d_fastd) VD_CUDA(cudaMalloc(&c.d_fastd, nb * sizeof(double)));
-    vd_status st = ensure_scratch(&c, 3 * n * sizeof(double));
+    vd_status st = VD_OK;
+    if (!c.d_fast && (st = dev_alloc(c, &c.d_fast, nb * sizeof(float), "pair tables")) != VD_OK) return st;
+    if (!c.d_smooth && (st = dev_alloc(c, &c.d_smooth, nb * sizeof(float4), "pair tables")) != VD_OK) return st;
+    if (!c.d_fastd && (st = dev_alloc(c, &c.d_fastd, nb * sizeof(double), "pair tables")) != VD_OK) return st;
+    st = ensure_scratch(&c, 3 * n * sizeof(double));
     if (st != VD_OK) return st;
     TableParams p{};
     for (int k = 0; k < 6; ++k) p.w[k] = w[k];

@@ -55,12 +55,12 @@ class Stats(C.Structure):
     _fields_ = [("bfgs_evals", C.c_int64), ("grid_ms", C.c_double), ("dock_ms", C.c_double),
                 ("post_ms", C.c_double), ("dock_warps_per_block", C.c_int32), ("dock_blocks", C.c_int32),
                 ("dock_shape", C.c_int32), ("grid_shape", C.c_int32), ("graph_launches", C.c_int64),
-                ("graph_instantiations", C.c_int64), ("scoring_ms", C.c_double)]
+                ("graph_instantiations", C.c_int64), ("scoring_ms", C.c_double), ("device_bytes", C.c_int64)]
 
 
 EXPORTS = [
-    "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_scoring", "vd_set_scoring_device",
-    "vd_set_receptor",
+    "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_memory_cap", "vd_set_scoring",
+    "vd_set_scoring_device", "vd_set_receptor",
     "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
     "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
     "vd_pose_coords",
@@ -82,6 +82,7 @@ def lib():
         L.vd_get_stats.argtypes = [_vp, C.POINTER(Stats)]
         L.vd_set_scoring.argtypes = [_vp, _dp]
         L.vd_set_scoring_device.argtypes = [_vp, _dp]
+        L.vd_set_memory_cap.argtypes = [_vp, C.c_int64]
         L.vd_set_receptor.argtypes = [_vp, C.c_int32, _dp, _ip]
         L.vd_set_box.argtypes = [_vp, _dp, _dp]
         L.vd_grid_dims.argtypes = [_vp, _ip, _dp, _dp]
@@ -105,7 +106,7 @@ def lib():
         L.vd_refine.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.c_int32, _fp]
         L.vd_score.argtypes = [_vp, C.c_int32, C.c_int32, _fp, _fp, _fp]
         L.vd_get_tables.argtypes = [_vp, _dp, _dp, _dp]
-        for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_scoring", "vd_set_scoring_device",
+        for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_memory_cap", "vd_set_scoring", "vd_set_scoring_device",
                      "vd_set_receptor",
                      "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand",
                      "vd_ligand_info", "vd_clear_ligands", "vd_energy", "vd_energy_grad",
@@ -185,6 +186,10 @@ class Context:
         s = Stats()
         _check(self.L.vd_get_stats(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def set_memory_cap(self, nbytes):
+        """Cap on the context's device memory (0 = none); past it calls raise with status 6."""
+        _check(self.L.vd_set_memory_cap(self.h, int(nbytes)))
 
     def set_scoring(self, weights, device=False):
         """New scoring weights (gauss1, gauss2, repulsion, hydrophobic, hydrogen,
