@@ -35,6 +35,17 @@ def test_library_exports_every_declared_entry_point(lib):
     assert set(vdock.EXPORTS) <= set(names)
 
 
+def test_checked_build_exports_the_same_entry_points():
+    """libvdock_checked.so (make checked: device bounds checks) is a drop-in
+    for libvdock.so: it loads without a GPU and exports every declared call."""
+    path = os.path.join(REPO, "vina-cuda_b200", "libvdock_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("checked build not made (make -C vina-cuda_b200 checked)")
+    checked = C.CDLL(path)
+    for n in header_functions():
+        assert hasattr(checked, n), n
+
+
 def fixture_text(golden_dir, name):
     return gzip.open(os.path.join(golden_dir, "pdbqt", name + ".gz"), "rt").read()
 

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
             item = __shfl_sync(0xffffffffu, v, 0);
         }
         if (item >= p.total_items) break;
-        const int li = find_ligand(p.prefix, p.n_ligs, item);
+        const int li = VD_DCLAMP(find_ligand(p.prefix, p.n_ligs, item), 0, p.n_ligs - 1, kChkItem);
         const uint32_t chain = uint32_t(item - __ldg(&p.prefix[li]));
         const LigView L = lig_view(p.pool, __ldg(&p.lig_off[li]));
         const int nc = 7 + L.nt, nc4 = pad4(nc);
@@ -300,6 +300,12 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
 
 }  // namespace vd
 
+namespace vd {
+// the docking kernel's check word lives in this file; launches from other
+// files (the batched pipeline) read it through here
+vd_status dock_take_checks(const char* where) { return take_device_checks(where); }
+}  // namespace vd
+
 using namespace vd;
 
 extern "C" {
@@ -320,6 +326,7 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
     unsigned long long ev = 0;
     VD_CUDA(cudaMemcpyAsync(&ev, c.d_counter + 2, 8, cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaStreamSynchronize(c.stream));
+    if ((st = take_device_checks("docking kernel")) != VD_OK) return st;
     float ms = 0;
     VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.dock_ms = ms;

@@ -38,5 +38,8 @@ vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_para
                       DockBuffers& out, cudaStream_t stream);
 // Feeds the kernel time per search evaluation of a finished launch to the autotuner.
 void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals);
+// Reads and clears the docking kernel's device bounds-check word (checked
+// build only; VD_OK otherwise).
+vd_status dock_take_checks(const char* where);
 
 }  // namespace vd

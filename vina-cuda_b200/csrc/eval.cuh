@@ -22,6 +22,7 @@
 // atomics are issued in a fixed program order by a single warp.
 #pragma once
 
+#include "checks.cuh"
 #include "common.h"
 
 namespace vd {
@@ -157,7 +158,7 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
             P = *reinterpret_cast<const float4*>(m.nd + kNodeF * k + kNdAA);
             const NodeRec& nk = L.nodes[k];
             w = make_float3(__ldg(&nk.rel_origin[0]), __ldg(&nk.rel_origin[1]), __ldg(&nk.rel_origin[2]));
-            int j = __ldg(&nk.parent);
+            int j = VD_DCLAMP(__ldg(&nk.parent), 0, k - 1, kChkParent);
             while (j > 0) {
                 const float4 aj = *reinterpret_cast<const float4*>(m.nd + kNodeF * j + kNdAA);
                 const NodeRec& nj = L.nodes[j];
@@ -165,7 +166,7 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
                 w = make_float3(__ldg(&nj.rel_origin[0]) + r.x, __ldg(&nj.rel_origin[1]) + r.y,
                                 __ldg(&nj.rel_origin[2]) + r.z);
                 P = qmul(aj, P);
-                j = __ldg(&nj.parent);
+                j = VD_DCLAMP(__ldg(&nj.parent), 0, j - 1, kChkParent);
             }
         }
         float4 q = qmul(qr, P);
@@ -181,7 +182,7 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
     // 3a: heavy-atom coordinates
     for (int i = lane; i < L.na; i += 32) {
         const float4 a = __ldg(&L.atoms[i]);
-        const int k = (__float_as_int(a.w) >> 8) & 0xff;
+        const int k = VD_DCLAMP((__float_as_int(a.w) >> 8) & 0xff, 0, L.nn - 1, kChkAtomBody);
         const float4* nd = reinterpret_cast<const float4*>(m.nd + kNodeF * k);
         const float4 r0 = nd[0], r1 = nd[1], r2 = nd[2];
         m.c[i] = make_float4(r0.w + (r0.x * a.x + r0.y * a.y + r0.z * a.z),
@@ -243,6 +244,13 @@ struct GridInter {
     float v, slope;
     __device__ __forceinline__ float operator()(int t, float px, float py, float pz, float& gx, float& gy,
                                                 float& gz) const {
+#ifdef VD_CHECKS
+        if (t < 0 || t >= kTypes || !G->map[t]) {
+            VD_DCHECK(false, kChkMapMissing);
+            gx = gy = gz = 0.f;
+            return 0.f;
+        }
+#endif
         return grid_term(*G, G->map[t], px, py, pz, v, slope, gx, gy, gz);
     }
 };
@@ -282,7 +290,10 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const bool two = p + 1 < p1;
             const int2 q0 = __ldg(&L.pairs[p]);
             const int2 q1 = two ? __ldg(&L.pairs[p + 1]) : q0;
-            const int a0 = q0.x & 0xffff, b0 = q0.x >> 16, a1 = q1.x & 0xffff, b1 = q1.x >> 16;
+            const int a0 = VD_DCLAMP(q0.x & 0xffff, 0, L.na - 1, kChkPairAtom);
+            const int b0 = VD_DCLAMP(q0.x >> 16, 0, L.na - 1, kChkPairAtom);
+            const int a1 = VD_DCLAMP(q1.x & 0xffff, 0, L.na - 1, kChkPairAtom);
+            const int b1 = VD_DCLAMP(q1.x >> 16, 0, L.na - 1, kChkPairAtom);
             if (b0 != cur_b) {  // b repeats along the segment: its coordinates stay in registers
                 flush(b0);
                 cb = m.c[b0];
@@ -293,11 +304,14 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
             const float d0 = r0x * r0x + r0y * r0y + r0z * r0z, d1 = r1x * r1x + r1y * r1y + r1z * r1z;
             const float rf0 = fminf(32.f * d0, 2047.5f), rf1 = fminf(32.f * d1, 2047.5f);
-            const int i0 = int(rf0), i1 = int(rf1);
+            const int i0 = VD_DCLAMP(int(rf0), 0, kBins - 2, kChkTableBin);
+            const int i1 = VD_DCLAMP(int(rf1), 0, kBins - 2, kChkTableBin);
+            const int tp0 = VD_DCLAMP(q0.y, 0, kPairTypes - 1, kChkPairType);
+            const int tp1 = VD_DCLAMP(q1.y, 0, kPairTypes - 1, kChkPairType);
             const bool in0 = d0 < 64.f, in1 = two && d1 < 64.f;
             float4 t0 = make_float4(0.f, 0.f, 0.f, 0.f), t1 = t0;
-            if (in0) t0 = __ldg(smooth + size_t(q0.y) * kBins + i0);  // no gather past the cutoff
-            if (in1) t1 = __ldg(smooth + size_t(q1.y) * kBins + i1);
+            if (in0) t0 = __ldg(smooth + size_t(tp0) * kBins + i0);  // no gather past the cutoff
+            if (in1) t1 = __ldg(smooth + size_t(tp1) * kBins + i1);
             const float w0 = rf0 - float(i0), w1 = rf1 - float(i1);
             float e0 = t0.x + w0 * (t0.z - t0.x), g0 = t0.y + w0 * (t0.w - t0.y);
             float e1 = t1.x + w1 * (t1.z - t1.x), g1 = t1.y + w1 * (t1.w - t1.y);
@@ -389,7 +403,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     __syncwarp();
     // 7: subtree sums (prefix differences), torques and the pose gradient
     for (int k = lane; k < L.nn; k += 32) {
-        const int b = __ldg(&L.nodes[k].atom_begin), e1 = __ldg(&L.nodes[k].sub_atom_end);
+        const int e1 = VD_DCLAMP(__ldg(&L.nodes[k].sub_atom_end), 0, L.na, kChkSubtree);
+        const int b = VD_DCLAMP(__ldg(&L.nodes[k].atom_begin), 0, e1, kChkSubtree);
         const int a4 = pad4(L.na);
         float F0 = 0.f, F1 = 0.f, F2 = 0.f, M0 = 0.f, M1 = 0.f, M2 = 0.f;
         if (e1 > b) {

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "checks.cuh"
 #include "common.h"
 
 namespace vd {
@@ -151,6 +152,7 @@ __global__ void __launch_bounds__(32 * TZ, 16 / TZ) grid_build_kernel(GridParams
     }
     const int ry = max(0, c_hi[1] - c_lo[1] + 1), rz = max(0, c_hi[2] - c_lo[2] + 1);
     // rows <= kMaxRows: the host checks the tile span against the cell size
+    VD_DCHECK(c_lo[0] > c_hi[0] || ry * rz <= kMaxRows, kChkGridRows);
     const int n_rows = (c_lo[0] <= c_hi[0]) ? min(kMaxRows, ry * rz) : 0;
     const int n_combo = p.n_rtypes * n_rows;  // (receptor type, row), type-major
 
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(32 * TZ, 16 / TZ) grid_build_kernel(GridParams
                 // Every point loads a row; points beyond the cutoff read the
                 // type's zero row (always an L1 hit), so the four loads issue
                 // back to back instead of behind one branch each.
-                const float* row_base = p.lut + at.type * (kLutRows * NTG);
+                const float* row_base = p.lut + VD_DCLAMP(at.type, 0, p.n_rtypes - 1, kChkGridType) * (kLutRows * NTG);
                 int bin[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
@@ -417,6 +419,7 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
         }
         VD_CUDA(cudaEventRecord(c.ev1, c.stream));
         VD_CUDA(cudaEventSynchronize(c.ev1));
+        if ((st = take_device_checks("grid kernel")) != VD_OK) return st;
         float ms = 0;
         VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
         c.grid_tune.pick(key, 2);

@@ -175,6 +175,7 @@ static vd_status pose_host(vd_ctx* h, int32_t lig, int32_t n, const float* poses
     unsigned long long ev = 0;
     if (mode == 3) VD_CUDA(cudaMemcpyAsync(&ev, c.d_counter + 8, 8, cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaStreamSynchronize(c.stream));
+    { const vd_status cs = take_device_checks("pose kernel"); if (cs != VD_OK) return cs; }
     if (evals) *evals = int64_t(ev);
     c.stats.bfgs_evals += int64_t(ev) + (mode == 1 ? n : 0);
     return VD_OK;

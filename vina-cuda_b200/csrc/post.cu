@@ -47,7 +47,7 @@ __device__ __forceinline__ int cell_of(const RecView& R, double x, double y, dou
         const int mx = R.dim[d] - 1;
         idx[d] = (t <= 0) ? 0 : ((t >= mx) ? mx : min(int(t), mx));
     }
-    return idx[0] + R.dim[0] * (idx[1] + R.dim[1] * idx[2]);
+    return VD_DCLAMP(idx[0] + R.dim[0] * (idx[1] + R.dim[1] * idx[2]), 0, R.dim[0] * R.dim[1] * R.dim[2] - 1, kChkCell);
 }
 
 // non_cache::eval_deriv term of one atom (FP32), smooth table, curl v.
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(256) cluster_kernel(ClusterParams p) {
     for (int r = 0; r < n && nk < p.max_keep; ++r) {
         const unsigned long long k = keys[r];
         if (k == ~0ull) break;
-        const int item = b0 + int(uint32_t(k));
+        const int item = b0 + VD_DCLAMP(int(uint32_t(k)), 0, n - 1, kChkClusterKept);
         for (int i = lane; i < nc; i += 32) m.x[i] = p.conf[size_t(item) * p.stride + i];
         __syncwarp();
         kinematics(L, m, lane);
@@ -954,6 +954,8 @@ vd_status dock_pipeline(Ctx& c, const std::vector<int>& ligs, const vd_search_pa
         if (st != VD_OK) return st;
     }
     VD_CUDA(cudaStreamSynchronize(c.stream));
+    if ((st = dock_take_checks("docking kernel")) != VD_OK) return st;
+    if ((st = take_device_checks("post-processing kernels")) != VD_OK) return st;
     float dock_ms = 0, post_ms = 0;
     VD_CUDA(cudaEventElapsedTime(&dock_ms, c.ev0, c.ev1));
     VD_CUDA(cudaEventElapsedTime(&post_ms, c.ev1, c.ev2));
@@ -1051,6 +1053,7 @@ vd_status vd_refine(vd_ctx* h, int32_t lig, int32_t n, float* poses, int32_t max
     VD_CUDA(cudaMemcpyAsync(poses, d_p, size_t(n) * nc * 4, cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaMemcpyAsync(e_out, d_e, n * 4, cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaStreamSynchronize(c.stream));
+    { const vd_status cs = take_device_checks("refinement kernel"); if (cs != VD_OK) return cs; }
     return VD_OK;
 }
 
@@ -1081,6 +1084,7 @@ vd_status vd_score(vd_ctx* h, int32_t lig, int32_t n, const float* poses, float*
     std::vector<double> o(size_t(n) * 2);
     VD_CUDA(cudaMemcpyAsync(o.data(), d_o, o.size() * 8, cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaStreamSynchronize(c.stream));
+    { const vd_status cs = take_device_checks("scoring kernel"); if (cs != VD_OK) return cs; }
     for (int i = 0; i < n; ++i) {
         if (adjusted) adjusted[i] = float(o[2 * i]);
         if (intra) intra[i] = float(o[2 * i + 1]);
