@@ -48,7 +48,12 @@ void set_error(const std::string& msg);
 
 // ---------------------------------------------------------------- device ligand
 // One ligand is one contiguous blob of 16-byte words in the ligand pool:
-//   LigHeader | atoms (float4) | nodes (NodeRec) | pairs (int2)
+//   LigHeader | atoms (float4) | nodes (NodeRec) | pairs (int2) | lane pairs (int4)
+// The lane-pair array holds the same pairs split into the 32 per-lane
+// segments the energy kernel walks (lane l: pairs [l*P/32, (l+1)*P/32) of the
+// ordered list), two pairs per int4, interleaved so that iteration k of every
+// lane reads entry k*32 + l: one coalesced 512-byte warp load per two pairs.
+// A lane's odd last pair is repeated in the int4's second half.
 // Only heavy atoms (XS type >= 0) are on the device; hydrogens carry no
 // energy and are placed on the host when output files are written.
 struct LigHeader {
@@ -60,7 +65,9 @@ struct LigHeader {
     int32_t off_nodes;
     int32_t off_pairs;    // int2 entries start (16-byte word offset)
     int32_t max_depth;
-    int32_t pad0, pad1, pad2, pad6;
+    int32_t off_lpairs;   // lane-pair int4 entries start (16-byte word offset)
+    int32_t lp_iters;     // int4 entries per lane (longest segment, two pairs each)
+    int32_t pad2, pad6;
     float num_tors;       // N_tors of the conf-independent term
     float pad3, pad4, pad5;
 };

@@ -7,7 +7,7 @@
 //      (rotation about a body-fixed axis; equals tree.h:282-292)
 //   3. lanes = atoms: coordinates, trilinear grid term (grid.cpp:50-160)
 //   4. lanes = segments of the pair list sorted by second atom, two pairs
-//      per iteration: intra pair term; the force on the second atom is
+//      per iteration (read from the lane-interleaved copy): intra pair term; the force on the second atom is
 //      accumulated in registers, the force on the first atom is added with a
 //      shared-memory atomic (model.cpp:1241-1256)
 //   6. lanes = contiguous atom ranges: warp prefix sums over the heavy atoms
@@ -42,6 +42,7 @@ struct LigView {
     const float4* atoms;
     const NodeRec* nodes;
     const int2* pairs;
+    const int4* lpairs;         // per-lane segments, two pairs per entry, interleaved by lane
     int32_t na, nn, np, nt;
     float num_tors;
 };
@@ -58,6 +59,7 @@ __device__ __forceinline__ LigView lig_view(const float4* pool, int64_t off) {
     L.atoms = b + h->off_atoms;
     L.nodes = reinterpret_cast<const NodeRec*>(b + h->off_nodes);
     L.pairs = reinterpret_cast<const int2*>(b + h->off_pairs);
+    L.lpairs = reinterpret_cast<const int4*>(b + h->off_lpairs);
     return L;
 }
 
@@ -275,7 +277,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     // force on a with an atomic.  Table indices are clamped and pairs past
     // the cutoff masked (their table loads predicated off).
     {
-        const int p0 = (lane * L.np) >> 5, p1 = ((lane + 1) * L.np) >> 5;
+        const int len = (((lane + 1) * L.np) >> 5) - ((lane * L.np) >> 5);
+        const int4* lp = L.lpairs + lane;
         int cur_b = -1;
         float bx = 0.f, by = 0.f, bz = 0.f;
         auto flush = [&](int nb) {
@@ -286,10 +289,11 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             bx = by = bz = 0.f;
         };
         float4 cb = make_float4(0.f, 0.f, 0.f, 0.f);  // coordinates of cur_b
-        for (int p = p0; p < p1; p += 2) {
-            const bool two = p + 1 < p1;
-            const int2 q0 = __ldg(&L.pairs[p]);
-            const int2 q1 = two ? __ldg(&L.pairs[p + 1]) : q0;
+        for (int p = 0; p < len; p += 2, lp += 32) {
+            const bool two = p + 1 < len;
+            const int4 qq = __ldg(lp);  // coalesced across the warp
+            const int2 q0 = make_int2(qq.x, qq.y);
+            const int2 q1 = two ? make_int2(qq.z, qq.w) : q0;
             const int a0 = VD_DCLAMP(q0.x & 0xffff, 0, L.na - 1, kChkPairAtom);
             const int b0 = VD_DCLAMP(q0.x >> 16, 0, L.na - 1, kChkPairAtom);
             const int a1 = VD_DCLAMP(q1.x & 0xffff, 0, L.na - 1, kChkPairAtom);

@@ -212,7 +212,19 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     H.off_atoms = 4;
     H.off_nodes = H.off_atoms + nh;
     H.off_pairs = H.off_nodes + 3 * nn;
-    const int32_t total = H.off_pairs + std::max<int32_t>(1, words(size_t(P) * sizeof(int2)));
+    H.off_lpairs = H.off_pairs + std::max<int32_t>(1, words(size_t(P) * sizeof(int2)));
+    int max_seg = 0;
+    for (int l = 0; l < 32; ++l) max_seg = std::max(max_seg, ((l + 1) * P >> 5) - (l * P >> 5));
+    H.lp_iters = (max_seg + 1) / 2;
+    std::vector<int4> lpairs(size_t(32) * H.lp_iters, make_int4(0, 0, 0, 0));
+    for (int l = 0; l < 32; ++l) {
+        const int p0 = l * P >> 5, p1 = (l + 1) * P >> 5;
+        for (int p = p0, k = 0; p < p1; p += 2, ++k) {
+            const int2 q0 = pairs[p], q1 = p + 1 < p1 ? pairs[p + 1] : q0;
+            lpairs[size_t(k) * 32 + l] = make_int4(q0.x, q0.y, q1.x, q1.y);
+        }
+    }
+    const int32_t total = H.off_lpairs + std::max<int32_t>(1, int32_t(lpairs.size()));
     H.num_tors = float(d->num_tors);
     L.blob.assign(size_t(total), make_float4(0, 0, 0, 0));
     char* base = reinterpret_cast<char*>(L.blob.data());
@@ -220,6 +232,7 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     std::memcpy(base + 16 * size_t(H.off_atoms), atoms.data(), atoms.size() * sizeof(float4));
     std::memcpy(base + 16 * size_t(H.off_nodes), nodes.data(), nodes.size() * sizeof(NodeRec));
     if (P) std::memcpy(base + 16 * size_t(H.off_pairs), pairs.data(), pairs.size() * sizeof(int2));
+    if (!lpairs.empty()) std::memcpy(base + 16 * size_t(H.off_lpairs), lpairs.data(), lpairs.size() * sizeof(int4));
     L.heavy_index = heavy_index;
     L.n_all_atoms = na;
     L.num_tors = d->num_tors;
