@@ -7,9 +7,14 @@
 //      (rotation about a body-fixed axis; equals tree.h:282-292)
 //   3. lanes = atoms: coordinates, trilinear grid term (grid.cpp:50-160)
 //   4. lanes = segments of the pair list sorted by second atom, two pairs
-//      per iteration (read from the lane-interleaved copy): intra pair term; the force on the second atom is
-//      accumulated in registers, the force on the first atom is added with a
-//      shared-memory atomic (model.cpp:1241-1256)
+//      per iteration (read from the lane-interleaved copy): intra pair term;
+//      the force on the second atom is accumulated in registers, the force
+//      on the first atom is added with a shared-memory atomic
+//      (model.cpp:1241-1256).  Pair forces are summed in 32-bit fixed point
+//      (2^-19 kcal/mol/A): shared-memory 32-bit integer atomics are native,
+//      FP32 (and 64-bit) ones are compare-and-swap loops that serialise the
+//      lanes hitting one atom; integer sums are exact, so the result does not
+//      depend on the order in which the atomics land
 //   6. lanes = contiguous atom ranges: warp prefix sums over the heavy atoms
 //      of force and moment about the root origin
 //   7. lanes = bodies: subtree sums as differences of two prefixes (a
@@ -18,8 +23,7 @@
 //        dE/dtorsion = T_k . axis_k (the bottom-up recursion of
 //        tree.h:169-178, 341-348, 373-422)
 //   8. warp butterfly sum of the energy (deterministic).
-// The per-body and subtree sums run in a fixed order; the pair-force
-// atomics are issued in a fixed program order by a single warp.
+// The per-body and subtree sums run in a fixed order.
 #pragma once
 
 #include "checks.cuh"
@@ -79,8 +83,8 @@ struct WarpMem {
     float* x;
     float* nd;
     float4* c;          // heavy-atom coordinates (w unused)
-    float *fx, *fy, *fz;
-    float* ns;          // [3][pad4(na)] prefix moments
+    float *fx, *fy, *fz;  // [pad4(na)] grid-term forces, then prefix forces
+    float* ns;          // [3][pad4(na)] fixed-point pair forces, then prefix moments
     float* g;
 };
 
@@ -97,6 +101,14 @@ __device__ __forceinline__ WarpMem carve(float* p, int na, int nn, int np, int n
     m.g = p;
     return m;
 }
+
+// Fixed point of the intra-pair forces: 2^19 units per kcal/mol/A.  A pair
+// force is the table slope (below 15 kcal/mol/A for the XS terms; the table
+// is capped and its derivative is zero at r = 0), so an atom's sum over at
+// most 127 partners stays inside the +-4096 range.
+constexpr float kFixScale = 524288.f;
+__device__ __forceinline__ int to_fixed(float v) { return __float2int_rn(v * kFixScale); }
+__device__ __forceinline__ float from_fixed(int v) { return float(v) * (1.f / kFixScale); }
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
@@ -268,7 +280,12 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         float gx, gy, gz;
         const float4 ci = m.c[i];
         e += inter(t, ci.x, ci.y, ci.z, gx, gy, gz);
-        if (want_grad) { m.fx[i] = gx; m.fy[i] = gy; m.fz[i] = gz; }
+        if (want_grad) {
+            int* const q = reinterpret_cast<int*>(m.ns);  // pair-force accumulators start at zero
+            const int a4 = pad4(L.na);
+            m.fx[i] = gx; m.fy[i] = gy; m.fz[i] = gz;
+            q[i] = 0; q[a4 + i] = 0; q[2 * a4 + i] = 0;
+        }
     }
     if (want_grad) __syncwarp();
     // 4: intra pairs.  Pairs are sorted by their second atom b; each lane
@@ -281,9 +298,13 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         const int4* lp = L.lpairs + lane;
         int cur_b = -1;
         float bx = 0.f, by = 0.f, bz = 0.f;
+        int* const qx = reinterpret_cast<int*>(m.ns);
+        int* const qy = qx + pad4(L.na);
+        int* const qz = qy + pad4(L.na);
         auto flush = [&](int nb) {
             if (want_grad && cur_b >= 0) {
-                atomicAdd(&m.fx[cur_b], bx); atomicAdd(&m.fy[cur_b], by); atomicAdd(&m.fz[cur_b], bz);
+                atomicAdd(&qx[cur_b], to_fixed(bx)); atomicAdd(&qy[cur_b], to_fixed(by));
+                atomicAdd(&qz[cur_b], to_fixed(bz));
             }
             cur_b = nb;
             bx = by = bz = 0.f;
@@ -333,7 +354,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             if (want_grad) {
                 if (in0) {
                     const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
-                    atomicAdd(&m.fx[a0], -Fx); atomicAdd(&m.fy[a0], -Fy); atomicAdd(&m.fz[a0], -Fz);
+                    atomicAdd(&qx[a0], to_fixed(-Fx)); atomicAdd(&qy[a0], to_fixed(-Fy)); atomicAdd(&qz[a0], to_fixed(-Fz));
                     bx += Fx; by += Fy; bz += Fz;
                 }
                 if (two) {
@@ -343,7 +364,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
                     }
                     if (in1) {
                         const float Fx = g1 * r1x, Fy = g1 * r1y, Fz = g1 * r1z;
-                        atomicAdd(&m.fx[a1], -Fx); atomicAdd(&m.fy[a1], -Fy); atomicAdd(&m.fz[a1], -Fz);
+                        atomicAdd(&qx[a1], to_fixed(-Fx)); atomicAdd(&qy[a1], to_fixed(-Fy)); atomicAdd(&qz[a1], to_fixed(-Fz));
                         bx += Fx; by += Fy; bz += Fz;
                     }
                 }
@@ -367,7 +388,9 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         float* mz = m.ns + 2 * a4;
         auto contrib = [&](int i, float v[6]) {
             const float4 ci = m.c[i];
-            const float fx = m.fx[i], fy = m.fy[i], fz = m.fz[i];
+            const int* q = reinterpret_cast<const int*>(m.ns);  // read before this lane overwrites it
+            const float fx = m.fx[i] + from_fixed(q[i]), fy = m.fy[i] + from_fixed(q[a4 + i]),
+                        fz = m.fz[i] + from_fixed(q[2 * a4 + i]);
             const float dx = ci.x - ox, dy = ci.y - oy, dz = ci.z - oz;
             v[0] = fx; v[1] = fy; v[2] = fz;
             v[3] = dy * fz - dz * fy;

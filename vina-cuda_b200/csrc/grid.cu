@@ -29,7 +29,7 @@ namespace vd {
 namespace {
 
 constexpr int kTileX = 16, kTileY = 8;  // z tile (TZ = 8 or 4) is a launch shape; threads = 32 * TZ
-constexpr int kStageCap = 1024;   // atoms staged per chunk (32 KB)
+constexpr int kStageCap = 128;    // atoms staged per chunk (4 KB; a 70 A tile keeps ~60, larger counts loop)
 constexpr double kCellSize = 4.0;
 constexpr int kLutRows = kBins + 1;  // table rows per receptor type; the last is zero
 
