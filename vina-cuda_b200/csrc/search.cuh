@@ -64,7 +64,17 @@ __device__ __forceinline__ float4 quat_increment(float4 q, float r0, float r1, f
 struct Vec2 {  // one lane's share of a pose-space vector
     float a, b;
 };
-__device__ __forceinline__ float vdot(Vec2 x, Vec2 y) { return warp_sum(x.a * y.a + x.b * y.b); }
+__device__ __forceinline__ float lane_dot(Vec2 x, Vec2 y) { return x.a * y.a + x.b * y.b; }
+__device__ __forceinline__ float vdot(Vec2 x, Vec2 y) { return warp_sum(lane_dot(x, y)); }
+// N independent dot products in one butterfly: each sum takes the same
+// steps as warp_sum, so the values equal N separate vdot calls.
+template <int N>
+__device__ __forceinline__ void warp_sum_n(float (&v)[N]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int j = 0; j < N; ++j) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
+}
 __device__ __forceinline__ Vec2 vload(const float* g, int n, int lane) {
     Vec2 v;
     v.a = (lane < n) ? g[lane] : 0.f;
@@ -114,9 +124,9 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
     const float fx_orig = fx;
     copy_conf(s.m.x, s.xo, nc, lane);
     Vec2 d = {-g.a, -g.b};
-    float gg = vdot(g, g);
+    const float gg = vdot(g, g);  // = d.d (d = -g)
     if (!(sqrtf(gg) >= 1e-5f)) return fx;
-    float step = 1.f / sqrtf(vdot(d, d));
+    float step = 1.f / sqrtf(gg);
     int k = 1;
     for (;;) {
         copy_conf(s.m.x, s.xp, nc, lane);
@@ -157,16 +167,22 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
             fx = fxp;
             break;
         }
-        if (!(sqrtf(vdot(g, g)) >= 1e-5f)) return fx;
-        if (max_steps <= k) break;
-        ++k;
+        // the update's dot products that do not depend on one another, in one
+        // reduction: g.g, y.s, y.y, s.s, gp.gp and s.d with d = -g
         const Vec2 sv = {step * d.a, step * d.b};
         const Vec2 yv = {g.a - gp.a, g.b - gp.b};
-        const float ys = vdot(yv, sv), yy = vdot(yv, yv);
-        d = {-g.a, -g.b};
-        const float cau = vdot(sv, sv) * sqrtf(vdot(gp, gp)) * 1.0e-6f;
+        const Vec2 dn = {-g.a, -g.b};
+        float dots[6] = {lane_dot(g, g), lane_dot(yv, sv), lane_dot(yv, yv), lane_dot(sv, sv), lane_dot(gp, gp),
+                         lane_dot(sv, dn)};
+        warp_sum_n(dots);
+        if (!(sqrtf(dots[0]) >= 1e-5f)) return fx;
+        if (max_steps <= k) break;
+        ++k;
+        const float ys = dots[1], yy = dots[2];
+        d = dn;
+        const float cau = dots[3] * sqrtf(dots[4]) * 1.0e-6f;
         if (ys > cau) {
-            const float alpha = vdot(sv, d) / ys;
+            const float alpha = dots[5] / ys;
             d.a += alpha * yv.a; d.b += alpha * yv.b;
             const float sc = ys / yy;
             d.a *= sc; d.b *= sc;
