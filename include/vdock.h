@@ -89,9 +89,10 @@ typedef struct {
     double   min_rmsd;        /* cluster radius 1.0                            */
     int32_t  refine;          /* 1 = refine + rescore on the GPU (main.cpp:434)*/
     int32_t  launch_shape;    /* docking kernel shape: 0 = autotuned per
-                                 workload, 1/2/3 = 64/48/40 registers per
-                                 thread (8/10/12 blocks of 4 chains per SM);
-                                 results do not depend on it                */
+                                 workload, 1/2/3/4/5 = 64/48/40/80/128
+                                 registers per thread (8/10/12/6/4 blocks of
+                                 4 chains per SM); results do not depend on
+                                 it                                         */
 } vd_search_params;
 
 typedef struct {
@@ -112,7 +113,7 @@ typedef struct {
     double  post_ms;             /* last cluster+refine+rescore kernels time    */
     int32_t dock_warps_per_block;/* chains per block of the last docking launch  */
     int32_t dock_blocks;
-    int32_t dock_shape;          /* launch_shape of the last docking launch (1-3) */
+    int32_t dock_shape;          /* launch_shape of the last docking launch (1-5) */
     int32_t grid_shape;          /* grid tile of the last build: 1 = 16x8x8 points
                                     per 256 threads, 2 = 16x8x4 per 128         */
     int64_t graph_launches;      /* batched pipelines submitted as a CUDA graph */

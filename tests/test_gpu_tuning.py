@@ -63,7 +63,7 @@ def _dock_ctx(vd):
 def test_dock_shapes_are_bit_identical(vd):
     ctx, ligs = _dock_ctx(vd)
     ref = None
-    for shape in (1, 2, 3):
+    for shape in (1, 2, 3, 4, 5):
         sp = vd.search_params(seed=11, n_chains=300, search_depth=3, launch_shape=shape)
         poses, e, ev = ctx.mc_chains(ligs[1], sp)
         assert ctx.stats()["dock_shape"] == shape
@@ -76,7 +76,7 @@ def test_dock_shapes_are_bit_identical(vd):
 def test_batched_shapes_are_bit_identical_and_tuner_settles(vd):
     ctx, ligs = _dock_ctx(vd)
     outs = []
-    for shape in (1, 2, 3, 0, 0, 0, 0):
+    for shape in (1, 2, 3, 4, 5, 0, 0, 0, 0, 0, 0):
         sp = vd.search_params(seed=3, n_chains=200, search_depth=2, refine=1, launch_shape=shape)
         res = ctx.dock_batched(ligs, sp)
         outs.append((res, ctx.stats()["dock_shape"]))
@@ -84,10 +84,10 @@ def test_batched_shapes_are_bit_identical_and_tuner_settles(vd):
         for a, b in zip(res, outs[0][0]):
             assert np.array_equal(a["energy"], b["energy"]) and np.array_equal(a["pose"], b["pose"])
             assert a["bfgs_evals"] == b["bfgs_evals"]
-    # three exploring calls run the three shapes, then the tuned one repeats
-    explored = sorted(s for _, s in outs[3:6])
-    assert explored == [1, 2, 3]
-    assert outs[6][1] in (1, 2, 3)
+    # five exploring calls run the five shapes, then the tuned one repeats
+    explored = sorted(s for _, s in outs[5:10])
+    assert explored == [1, 2, 3, 4, 5]
+    assert outs[10][1] in (1, 2, 3, 4, 5)
 
 
 def test_batched_pipeline_replays_one_graph(vd):
@@ -112,7 +112,7 @@ def test_batched_pipeline_replays_one_graph(vd):
 def test_shapes_bit_identical_on_screen_sized_ligands(vd):
     """The same on ligands of the wide-box screen's size (30-45 heavy atoms,
     up to ~700 intra pairs) with the heuristic search depth: every result
-    and every ligand's evaluation count agree across the three shapes."""
+    and every ligand's evaluation count agree across the five shapes."""
     from vdock import synth
     xyz, xs = synth.receptor(2000, 30.0, 8)
     ctx = vd.Context()
@@ -121,7 +121,7 @@ def test_shapes_bit_identical_on_screen_sized_ligands(vd):
     ctx.build_grids(synth.TYPES8)
     ligs = [ctx.add_ligand(l) for l in synth.ligand_set(6, (30, 45), (6, 12), 17)]
     outs = []
-    for shape in (1, 2, 3):
+    for shape in (1, 2, 3, 4, 5):
         sp = vd.search_params(seed=9, n_chains=1000, search_depth=0, refine=1, launch_shape=shape)
         outs.append(ctx.dock_batched(ligs, sp))
     for res in outs[1:]:

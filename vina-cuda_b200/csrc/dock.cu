@@ -55,8 +55,11 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
     return lo;
 }
 
-// MINB: 4-warp blocks per SM the register budget targets (8/10/12 -> 64/48/40
-// registers per thread); the autotuner picks one per workload.
+// MINB: 4-warp blocks per SM the register budget targets (8/10/12/6/4 ->
+// 64/48/40/80/128 registers per thread); the autotuner picks one per
+// workload.  The small budgets keep more chains resident for large batches;
+// the large ones drop the register spills (ptxas: 188 bytes of spill stores
+// at 64, none at 128), which pays when a launch has few chains per SM.
 template <bool persistent, int MINB>
 __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
     extern __shared__ float4 smem4[];
@@ -133,6 +136,8 @@ DockFn dock_fn(int shape) {
     switch (shape) {
         case 1: return dock_kernel<persistent, 10>;
         case 2: return dock_kernel<persistent, 12>;
+        case 3: return dock_kernel<persistent, 6>;
+        case 4: return dock_kernel<persistent, 4>;
         default: return dock_kernel<persistent, 8>;
     }
 }

@@ -25,7 +25,7 @@ struct DockBuffers {
     std::function<cudaError_t(cudaStream_t)> launch;  // the kernel launch
 };
 
-constexpr int kDockShapes = 3;      // register budgets 64/48/40 per thread
+constexpr int kDockShapes = 5;      // register budgets 64/48/40/80/128 per thread
 
 void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps);
 // prepare_dock: host work and device layout (no stream operation);
