@@ -45,7 +45,8 @@ def args_():
     a.add_argument("--batch", type=int, default=64, help="ligands per step")
     a.add_argument("--chains", type=int, default=CHAINS)
     a.add_argument("--plain-ligands", type=int, default=8)
-    a.add_argument("--e2e-steps", type=int, default=2)
+    a.add_argument("--e2e-steps", type=int, default=0,
+                   help="timed batches re-run end to end (0 = all K, the same batches as the timed region)")
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--cpu-ligands", type=int, default=3, help="whole ligands per CPU sample step")
     a.add_argument("--no-configs", action="store_true", help="skip the plain / adjoint / uneven-batch lines")
@@ -471,7 +472,8 @@ def run_ours(a):
     # end to end through the public API with host buffers: ligand topologies
     # copied in (vd_add_ligand + pool upload), results read back
     e2e_times, h2d, d2h = [], 0, 0
-    for k in range(min(a.e2e_steps, K)):
+    n_e2e = K if a.e2e_steps <= 0 else min(a.e2e_steps, K)
+    for k in range(n_e2e):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx.clear_ligands()
@@ -479,11 +481,16 @@ def run_ours(a):
         res = ctx.dock_batched(eids, sp)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    blob_bytes = sum(64 + 16 * int((l["xs"] >= 0).sum()) + 48 * len(l["node_parent"]) + 16 * len(l["pairs"]) +
-                     4 * int((l["xs"] >= 0).sum()) for l in (ligs[i] for i in batches[W]))
-    h2d = blob_bytes
+    def blob_bytes(lig):  # the ligand's pool blob (ligand.cpp layout), uploaded once per call
+        heavy, nn, npairs = int((lig["xs"] >= 0).sum()), len(lig["node_parent"]), len(lig["pairs"])
+        lp_iters = ((npairs + 31) // 32 + 1) // 2
+        return 16 * (4 + heavy + 3 * nn + max(1, (npairs + 1) // 2) + max(1, 32 * lp_iters))
+    h2d = int(sum(blob_bytes(ligs[i]) for k in range(n_e2e) for i in batches[W + k]) / max(1, n_e2e))
     d2h = B * 2 * 1024  # vd_dock_result per ligand
-    e2e_value = B * world / statistics.median(e2e_times) if e2e_times else None
+    e2e_total = sum(e2e_times)
+    if pg:
+        e2e_total = multi.max_over_ranks(e2e_total, device="cuda")
+    e2e_value = B * n_e2e * world / e2e_total if e2e_times else None
     if rank != 0:
         return
     hbm, src = peaks()
