@@ -121,6 +121,9 @@ typedef struct {
     double  scoring_ms;          /* wall time of the last vd_set_scoring(_device) */
     int64_t device_bytes;        /* device memory the context holds for maps, tables,
                                     ligands, receptor cells and scratch           */
+    double  pair_force_scale;    /* fixed-point units per kcal/mol/A in which the
+                                    kernels sum intra-pair forces (a power of two
+                                    set from the current tables; 2^19 by default) */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */

@@ -58,3 +58,57 @@ def test_device_tables_match_host_tables(vd):
         assert np.max(np.abs(eh - ed) / np.maximum(np.abs(eh), 1.0)) <= 1e-5
         assert np.max(np.abs(gh_ - gd_)) <= 1e-5 * max(1.0, np.abs(gh_).max())
     print("scoring ms (host, device):", times)
+
+
+def _expected_scale(sd):
+    """The library's rule (tables.cpp pair_force_scale): the largest power of
+    two, at most 2^24, for which 128 x the largest pair force (derivative
+    entry x r at the bin's upper end) stays below 2^30."""
+    r = np.sqrt(np.arange(1, 2049) / 32.0)
+    bound = (np.maximum(np.abs(sd[:, :2048]), np.abs(sd[:, 1:2049])) * r).max()
+    k = 24
+    while k > -24 and 128.0 * bound * 2.0 ** k >= 2.0 ** 30:
+        k -= 1
+    return 2.0 ** k
+
+
+def test_pair_force_scale_follows_the_weights(vd):
+    """Pair forces are summed in fixed point whose scale comes from the
+    tables: 2^19 for the default weights; forty-fold weights (pair forces up
+    to ~400 kcal/mol/A) lower it so no atom's sum can overflow, and energies
+    and gradients still match the oracle built with the same weights (the
+    parity tolerances: 1e-3 kcal/mol per unit of |e| above 1 for in-box poses,
+    gradients 1e-3 of |g|_inf)."""
+    import oracle_lib as O
+    from vdock import synth
+    xyz, xs = synth.receptor(1500, 25.0, 6)
+    lig = synth.ligand(36, 8, 5)
+    ctx = vd.Context()
+    ctx.set_receptor(xyz, xs)
+    ctx.set_box([0.0, 0.0, 0.0], [18.0] * 3)
+    assert ctx.stats()["pair_force_scale"] == 2.0 ** 19
+    big = [40.0 * w for w in DEFAULT[:5]] + [DEFAULT[5]]
+    orc = O.Oracle(weights=tuple(big))
+    ctx.set_scoring(big)
+    scale = ctx.stats()["pair_force_scale"]
+    assert scale == _expected_scale(orc.tables()[2]) and scale < 2.0 ** 19
+    for o in (orc,):
+        o.set_receptor(xyz, xs)
+        o.set_box([0.0, 0.0, 0.0], [18.0] * 3)
+    types = sorted(set(int(t) for t in lig["xs"]))
+    ctx.build_grids(types)
+    orc.build_grids(types)
+    lc, lo = ctx.add_ligand(lig), orc.add_ligand(lig)
+    poses = synth.random_poses(64, ctx.ntors[lc], -4.0, 4.0, seed=12)
+    e, g = ctx.energy_grad(lc, poses)
+    _, bmin, bmax = orc.grid_info()
+    checked = 0
+    for i, p in enumerate(poses):
+        x = orc.coords(lo, p.astype(np.float64), lig["n_atoms"])
+        if np.any((x < bmin) | (x > bmax)):
+            continue
+        e_ref, g_ref = orc.eval_deriv(lo, p.astype(np.float64))
+        assert abs(e[i] - e_ref) <= 1e-3 * max(1.0, abs(e_ref)), (i, e[i], e_ref)
+        assert np.abs(g[i] - g_ref).max() <= 1e-3 * max(1.0, np.abs(g_ref).max()), i
+        checked += 1
+    assert checked >= 16

@@ -217,3 +217,21 @@ def test_score_only_term_breakdown_is_consistent(golden_dir):
                 assert abs(e2 - e) <= 0.05, (name, e, e2, terms)
     assert n >= 300
     print(f"score_only breakdown: {n} poses, worst |sum w*term - affinity| = {worst:.4f}")
+
+
+def test_default_pair_forces_fit_the_fixed_point_range():
+    """The kernels sum intra-pair forces per atom in 32-bit fixed point, at
+    the largest power-of-two scale for which 128 x the tables' largest pair
+    force stays below 2^30 (tables.cpp pair_force_scale).  For the default
+    weights the largest pair force (derivative entry x r at the bin's upper
+    end) is ~10 kcal/mol/A, giving 2^19 units per kcal/mol/A with a 2x
+    margin to the 2^31 limit even for a 128-atom ligand."""
+    f, e, sd = O.Oracle().tables()
+    r = np.sqrt(np.arange(1, 2049) / 32.0)
+    bound = (np.maximum(np.abs(sd[:, :2048]), np.abs(sd[:, 1:2049])) * r).max()
+    assert 5.0 < bound < 15.0, bound
+    k = 24
+    while 128.0 * bound * 2.0 ** k >= 2.0 ** 30:
+        k -= 1
+    assert k == 19
+    assert 127 * bound * 2.0 ** k < 2.0 ** 31

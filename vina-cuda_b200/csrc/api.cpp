@@ -147,6 +147,7 @@ vd_status vd_set_memory_cap(vd_ctx* h, int64_t bytes) {
 vd_status vd_get_stats(vd_ctx* h, vd_stats* out) {
     VD_CHECK(h && out, VD_ERR_ARG, "vd_get_stats: NULL argument");
     h->c.stats.device_bytes = int64_t(h->c.dev_used);
+    h->c.stats.pair_force_scale = h->c.fix_scale;
     *out = h->c.stats;
     return VD_OK;
 }
@@ -154,6 +155,7 @@ vd_status vd_get_stats(vd_ctx* h, vd_stats* out) {
 // After new tables: maps built with the old weights are stale.
 static void scoring_changed(Ctx& c, std::chrono::steady_clock::time_point t0) {
     c.scoring = true;
+    c.fix_scale = pair_force_scale(c.sd);
     c.n_maps = 0;
     for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
     c.stats.scoring_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -161,6 +163,7 @@ static void scoring_changed(Ctx& c, std::chrono::steady_clock::time_point t0) {
 
 vd_status vd_set_scoring(vd_ctx* h, const double weights[6]) {
     VD_CHECK(h && weights, VD_ERR_ARG, "vd_set_scoring: NULL argument");
+    for (int i = 0; i < 6; ++i) VD_CHECK(std::isfinite(weights[i]), VD_ERR_ARG, "vd_set_scoring: non-finite weight");
     Ctx& c = h->c;
     const auto t0 = std::chrono::steady_clock::now();
     VD_CUDA(cudaSetDevice(c.device));
@@ -193,6 +196,8 @@ vd_status vd_set_scoring(vd_ctx* h, const double weights[6]) {
 
 vd_status vd_set_scoring_device(vd_ctx* h, const double weights[6]) {
     VD_CHECK(h && weights, VD_ERR_ARG, "vd_set_scoring_device: NULL argument");
+    for (int i = 0; i < 6; ++i)
+        VD_CHECK(std::isfinite(weights[i]), VD_ERR_ARG, "vd_set_scoring_device: non-finite weight");
     Ctx& c = h->c;
     const auto t0 = std::chrono::steady_clock::now();
     VD_CUDA(cudaSetDevice(c.device));

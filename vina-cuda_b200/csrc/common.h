@@ -116,6 +116,7 @@ struct Ctx {
     std::vector<double> fast, se, sd;     // [153][2051] double (host)
     float* d_fast = nullptr;              // [153][2049] float (rescoring, eval_fast)
     float4* d_smooth = nullptr;           // [153][2049] {e_i, dor_i, e_i+1, dor_i+1}
+    float fix_scale = 524288.f;           // fixed-point units per kcal/mol/A of the pair forces
     double* d_fastd = nullptr;            // [153][2049] double (final rescoring)
     // receptor
     std::vector<double> rec_xyz;
@@ -196,6 +197,10 @@ vd_status sync_pool(Ctx* c);
 vd_status ensure_receptor_cells(Ctx* c);
 void build_tables(const double w[6], std::vector<double>& fast, std::vector<double>& se,
                   std::vector<double>& sd);
+// Largest power of two (at most 2^24) for which 128 times the largest pair
+// force of the derivative table stays below 2^30: the fixed-point scale of
+// the kernels' per-atom pair-force sums.
+float pair_force_scale(const std::vector<double>& sd);
 // Same tables built on the device into the context's device copies, with
 // the double tables copied back to c.fast / c.se / c.sd.
 vd_status build_tables_device(Ctx& c, const double w[6]);

@@ -238,7 +238,7 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     p.n_ligs = n;
     p.total_items = items;
     p.smooth = c.d_smooth;
-    p.ep = {float(sp.hunt_cap[0]), float(sp.hunt_cap[1]), 1e6f};
+    p.ep = {float(sp.hunt_cap[0]), float(sp.hunt_cap[1]), 1e6f, c.fix_scale, 1.f / c.fix_scale};
     p.seed = sp.seed;
     p.temperature = float(sp.temperature > 0 ? sp.temperature : 1.2);
     p.amplitude = float(sp.amplitude > 0 ? sp.amplitude : 2.0);
@@ -439,7 +439,7 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     p.n_ligs = 1;
     p.total_items = n;
     p.smooth = c.d_smooth;
-    p.ep = {float(sp->hunt_cap[0]), float(sp->hunt_cap[1]), 1e6f};
+    p.ep = {float(sp->hunt_cap[0]), float(sp->hunt_cap[1]), 1e6f, c.fix_scale, 1.f / c.fix_scale};
     p.seed = sp->seed;
     p.temperature = float(sp->temperature > 0 ? sp->temperature : 1.2);
     p.amplitude = float(sp->amplitude > 0 ? sp->amplitude : 2.0);

@@ -11,7 +11,8 @@
 //      the force on the second atom is accumulated in registers, the force
 //      on the first atom is added with a shared-memory atomic
 //      (model.cpp:1241-1256).  Pair forces are summed in 32-bit fixed point
-//      (2^-19 kcal/mol/A): shared-memory 32-bit integer atomics are native,
+//      (EvalParams::fix units per kcal/mol/A, set from the tables so that
+//      no atom's sum can overflow): shared-memory 32-bit integer atomics are native,
 //      FP32 (and 64-bit) ones are compare-and-swap loops that serialise the
 //      lanes hitting one atom; integer sums are exact, so the result does not
 //      depend on the order in which the atomics land
@@ -40,6 +41,7 @@ struct MapView {
 
 struct EvalParams {
     float v_intra, v_inter, slope;
+    float fix, inv_fix;  // fixed-point units per kcal/mol/A of the pair forces (a power of two), 1/fix
 };
 
 struct LigView {
@@ -102,13 +104,12 @@ __device__ __forceinline__ WarpMem carve(float* p, int na, int nn, int np, int n
     return m;
 }
 
-// Fixed point of the intra-pair forces: 2^19 units per kcal/mol/A.  A pair
-// force is the table slope (below 15 kcal/mol/A for the XS terms; the table
-// is capped and its derivative is zero at r = 0), so an atom's sum over at
-// most 127 partners stays inside the +-4096 range.
-constexpr float kFixScale = 524288.f;
-__device__ __forceinline__ int to_fixed(float v) { return __float2int_rn(v * kFixScale); }
-__device__ __forceinline__ float from_fixed(int v) { return float(v) * (1.f / kFixScale); }
+// Fixed point of the intra-pair forces, `fix` units per kcal/mol/A: the
+// host picks the largest power of two for which 128 times the tables' largest
+// pair force stays below 2^30 (pair_force_scale), so an atom's sum over at
+// most 127 partners cannot overflow; 2^19 for the default weights.
+__device__ __forceinline__ int to_fixed(float v, float fix) { return __float2int_rn(v * fix); }
+__device__ __forceinline__ float from_fixed(int v, float inv_fix) { return float(v) * inv_fix; }
 
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
@@ -271,7 +272,7 @@ struct GridInter {
 
 template <bool want_grad, class Inter>
 __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const Inter& inter, const float4* smooth,
-                             float v_intra, int lane) {
+                             float v_intra, float fix, float inv_fix, int lane) {
     kinematics(L, m, lane);
     float e = 0.f;
     // 3b: grid term per atom; its gradient seeds the atom's force
@@ -303,8 +304,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         int* const qz = qy + pad4(L.na);
         auto flush = [&](int nb) {
             if (want_grad && cur_b >= 0) {
-                atomicAdd(&qx[cur_b], to_fixed(bx)); atomicAdd(&qy[cur_b], to_fixed(by));
-                atomicAdd(&qz[cur_b], to_fixed(bz));
+                atomicAdd(&qx[cur_b], to_fixed(bx, fix)); atomicAdd(&qy[cur_b], to_fixed(by, fix));
+                atomicAdd(&qz[cur_b], to_fixed(bz, fix));
             }
             cur_b = nb;
             bx = by = bz = 0.f;
@@ -354,7 +355,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             if (want_grad) {
                 if (in0) {
                     const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
-                    atomicAdd(&qx[a0], to_fixed(-Fx)); atomicAdd(&qy[a0], to_fixed(-Fy)); atomicAdd(&qz[a0], to_fixed(-Fz));
+                    atomicAdd(&qx[a0], to_fixed(-Fx, fix)); atomicAdd(&qy[a0], to_fixed(-Fy, fix));
+                    atomicAdd(&qz[a0], to_fixed(-Fz, fix));
                     bx += Fx; by += Fy; bz += Fz;
                 }
                 if (two) {
@@ -364,7 +366,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
                     }
                     if (in1) {
                         const float Fx = g1 * r1x, Fy = g1 * r1y, Fz = g1 * r1z;
-                        atomicAdd(&qx[a1], to_fixed(-Fx)); atomicAdd(&qy[a1], to_fixed(-Fy)); atomicAdd(&qz[a1], to_fixed(-Fz));
+                        atomicAdd(&qx[a1], to_fixed(-Fx, fix)); atomicAdd(&qy[a1], to_fixed(-Fy, fix));
+                    atomicAdd(&qz[a1], to_fixed(-Fz, fix));
                         bx += Fx; by += Fy; bz += Fz;
                     }
                 }
@@ -389,8 +392,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         auto contrib = [&](int i, float v[6]) {
             const float4 ci = m.c[i];
             const int* q = reinterpret_cast<const int*>(m.ns);  // read before this lane overwrites it
-            const float fx = m.fx[i] + from_fixed(q[i]), fy = m.fy[i] + from_fixed(q[a4 + i]),
-                        fz = m.fz[i] + from_fixed(q[2 * a4 + i]);
+            const float fx = m.fx[i] + from_fixed(q[i], inv_fix), fy = m.fy[i] + from_fixed(q[a4 + i], inv_fix),
+                        fz = m.fz[i] + from_fixed(q[2 * a4 + i], inv_fix);
             const float dx = ci.x - ox, dy = ci.y - oy, dz = ci.z - oz;
             v[0] = fx; v[1] = fy; v[2] = fz;
             v[3] = dy * fz - dz * fy;
@@ -468,7 +471,7 @@ template <bool want_grad>
 __device__ __forceinline__ float eval_pose(const LigView& L, const WarpMem& m, const MapView& G,
                                            const float4* smooth, const EvalParams ep, int lane) {
     const GridInter gi{&G, ep.v_inter, ep.slope};
-    return eval_pose_t<want_grad>(L, m, gi, smooth, ep.v_intra, lane);
+    return eval_pose_t<want_grad>(L, m, gi, smooth, ep.v_intra, ep.fix, ep.inv_fix, lane);
 }
 
 }  // namespace vd

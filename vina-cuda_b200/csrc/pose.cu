@@ -92,7 +92,7 @@ vd_status run_pose_kernel(Ctx& c, int lig, int n_poses, const float* d_poses, co
     p.smooth = c.d_smooth;
     const vd_eval_params def = {10.0, 10.0, 1e6};
     const vd_eval_params* e = ep ? ep : &def;
-    p.ep = {float(e->v_intra), float(e->v_inter), float(e->slope)};
+    p.ep = {float(e->v_intra), float(e->v_inter), float(e->slope), c.fix_scale, 1.f / c.fix_scale};
     p.poses = d_poses;
     p.n_poses = n_poses;
     p.e_out = d_e;

@@ -191,6 +191,7 @@ struct RefineParams {
     const int32_t* max_steps;   // per ligand (may be null)
     RecView R;
     const float4* smooth;
+    float fix, inv_fix;         // fixed-point scale of the pair forces (EvalParams::fix) and 1/fix
     int32_t warp_floats;
     unsigned long long* evals;
     int32_t skip_invalid;       // leave poses whose e_out is FLT_MAX untouched
@@ -199,11 +200,11 @@ struct RefineParams {
 // bfgs.h:95-140 (dense BFGS, Armijo backtracking), warp-parallel; H in smem.
 template <class Inter>
 __device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, float* gc, float* pv, float* yv,
-                           float* mhy, const Inter& inter, const float4* smooth, float v_intra, int max_steps,
-                           int lane, int& evals) {
+                           float* mhy, const Inter& inter, const float4* smooth, float v_intra, float fix,
+                           float inv_fix, int max_steps, int lane, int& evals) {
     const int n = 6 + L.nt, nc = 7 + L.nt;
     for (int i = lane; i < n * n; i += 32) H[i] = (i / n == i % n) ? 1.f : 0.f;
-    float f0 = eval_pose_t<true>(L, s.m, inter, smooth, v_intra, lane);
+    float f0 = eval_pose_t<true>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
     ++evals;
     for (int i = lane; i < n; i += 32) gc[i] = s.m.g[i];
     const float f_orig = f0;
@@ -221,7 +222,7 @@ __device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, floa
         float alpha = 1.f, f1 = 0.f;
         for (int trial = 0; trial < 10; ++trial) {  // line_search, bfgs.h:65-82
             conf_step(s.xp, s.m.x, p, alpha, L.nt, lane);
-            f1 = eval_pose_t<true>(L, s.m, inter, smooth, v_intra, lane);
+            f1 = eval_pose_t<true>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
             ++evals;
             if (f1 - f0 < 0.0001f * alpha * pg) break;
             alpha *= 0.5f;
@@ -298,7 +299,7 @@ __global__ void __launch_bounds__(32 * kRefineWarps) refine_kernel(RefineParams 
         for (int ramp = 0; ramp < 5; ++ramp) {
             const float slope = 100.f * powf(10.f, 2.f * ramp);
             const DirectInter di{&p.R, p.smooth, 1000.f, slope};
-            e = dense_bfgs(L, s, H, gc, pv, yv, mhy, di, p.smooth, 1000.f, max_steps, lane, evals);
+            e = dense_bfgs(L, s, H, gc, pv, yv, mhy, di, p.smooth, 1000.f, p.fix, p.inv_fix, max_steps, lane, evals);
             kinematics(L, s.m, lane);
             bool ok = true;  // non_cache::within, margin 1e-4
             for (int i = lane; i < L.na; i += 32) {
@@ -806,6 +807,8 @@ vd_status prepare_post(Ctx& c, const std::vector<int>& ligs, const vd_search_par
         rp.max_steps = d_steps;
         rp.R = rec_view(c);
         rp.smooth = c.d_smooth;
+        rp.fix = c.fix_scale;
+        rp.inv_fix = 1.f / c.fix_scale;
         rp.warp_floats = max_rwf;
         rp.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 4);
         rp.skip_invalid = 1;
@@ -1042,6 +1045,8 @@ vd_status vd_refine(vd_ctx* h, int32_t lig, int32_t n, float* poses, int32_t max
     rp.max_steps = nullptr;
     rp.R = rec_view(c);
     rp.smooth = c.d_smooth;
+    rp.fix = c.fix_scale;
+    rp.inv_fix = 1.f / c.fix_scale;
     rp.warp_floats = refine_warp_floats(L);
     rp.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 4);
     rp.skip_invalid = 0;

@@ -40,4 +40,18 @@ void build_tables(const double w[6], std::vector<double>& fast, std::vector<doub
         }
 }
 
+float pair_force_scale(const std::vector<double>& sd) {
+    // A pair force is the lerp of two derivative entries times r (at most
+    // r_{i+1} in bin i); the kernels sum up to 127 of them per atom.
+    double bound = 0.0;
+    for (int p = 0; p < kPairTypes; ++p)
+        for (int i = 0; i + 1 < kBins; ++i) {
+            const size_t b = size_t(p) * kN + i;
+            bound = std::fmax(bound, std::fmax(std::fabs(sd[b]), std::fabs(sd[b + 1])) * std::sqrt((i + 1) / 32.0));
+        }
+    int k = 24;  // finest scale used: 2^-24 kcal/mol/A
+    while (k > -24 && 128.0 * bound * std::ldexp(1.0, k) >= 1073741824.0) --k;
+    return float(std::ldexp(1.0, k));
+}
+
 }  // namespace vd
