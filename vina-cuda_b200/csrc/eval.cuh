@@ -367,7 +367,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
                     if (in1) {
                         const float Fx = g1 * r1x, Fy = g1 * r1y, Fz = g1 * r1z;
                         atomicAdd(&qx[a1], to_fixed(-Fx, fix)); atomicAdd(&qy[a1], to_fixed(-Fy, fix));
-                    atomicAdd(&qz[a1], to_fixed(-Fz, fix));
+                        atomicAdd(&qz[a1], to_fixed(-Fz, fix));
                         bx += Fx; by += Fy; bz += Fz;
                     }
                 }
