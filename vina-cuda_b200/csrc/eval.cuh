@@ -12,10 +12,10 @@
 //      on the first atom is added with a shared-memory atomic
 //      (model.cpp:1241-1256).  Pair forces are summed in 32-bit fixed point
 //      (EvalParams::fix units per kcal/mol/A, set from the tables so that
-//      no atom's sum can overflow): shared-memory 32-bit integer atomics are native,
-//      FP32 (and 64-bit) ones are compare-and-swap loops that serialise the
-//      lanes hitting one atom; integer sums are exact, so the result does not
-//      depend on the order in which the atomics land
+//      no atom's sum can overflow): on B200 shared-memory 32-bit integer
+//      atomics cost the same however many lanes hit one atom, FP32 (and
+//      64-bit) ones serialise those lanes; integer sums are exact, so the
+//      result does not depend on the order in which the atomics land
 //   6. lanes = contiguous atom ranges: warp prefix sums over the heavy atoms
 //      of force and moment about the root origin
 //   7. lanes = bodies: subtree sums as differences of two prefixes (a
