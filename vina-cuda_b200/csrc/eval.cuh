@@ -270,7 +270,12 @@ struct GridInter {
     }
 };
 
-template <bool want_grad, class Inter>
+// pair_atomics: the force on a pair's second atom also goes straight to its
+// accumulator with an atomic instead of being summed in registers along the
+// segment.  That is shorter and less divergent code, which the latency-bound
+// search prefers (+3-5%); the pose kernels, bound by L1 wavefronts, keep the
+// register sums (fewer atomics and coordinate loads, +14% there).
+template <bool want_grad, bool pair_atomics = false, class Inter>
 __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const Inter& inter, const float4* smooth,
                              float v_intra, float fix, float inv_fix, int lane) {
     kinematics(L, m, lane);
@@ -291,9 +296,10 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     if (want_grad) __syncwarp();
     // 4: intra pairs.  Pairs are sorted by their second atom b; each lane
     // takes a contiguous segment, two pairs at a time (two table gathers in
-    // flight), keeps b's force in registers while b repeats, and adds the
-    // force on a with an atomic.  Table indices are clamped and pairs past
-    // the cutoff masked (their table loads predicated off).
+    // flight), keeps b's coordinates and force in registers while b repeats
+    // (unless pair_atomics), and adds the force on a with an atomic.  Table
+    // indices are clamped and pairs past the cutoff masked (their table
+    // loads predicated off).
     {
         const int len = (((lane + 1) * L.np) >> 5) - ((lane * L.np) >> 5);
         const int4* lp = L.lpairs + lane;
@@ -320,11 +326,11 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const int b0 = VD_DCLAMP(q0.x >> 16, 0, L.na - 1, kChkPairAtom);
             const int a1 = VD_DCLAMP(q1.x & 0xffff, 0, L.na - 1, kChkPairAtom);
             const int b1 = VD_DCLAMP(q1.x >> 16, 0, L.na - 1, kChkPairAtom);
-            if (b0 != cur_b) {  // b repeats along the segment: its coordinates stay in registers
+            if (!pair_atomics && b0 != cur_b) {  // b repeats along the segment: its coordinates stay in registers
                 flush(b0);
                 cb = m.c[b0];
             }
-            const float4 cb0 = cb, cb1 = (b1 == b0) ? cb : m.c[b1];
+            const float4 cb0 = pair_atomics ? m.c[b0] : cb, cb1 = (pair_atomics || b1 != b0) ? m.c[b1] : cb;
             const float4 ca0 = m.c[a0], ca1 = m.c[a1];
             const float r0x = cb0.x - ca0.x, r0y = cb0.y - ca0.y, r0z = cb0.z - ca0.z;
             const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
@@ -348,11 +354,22 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             g0 = in0 ? g0 * c0 * c0 : 0.f;
             g1 = in1 ? g1 * c1 * c1 : 0.f;
             e += e0 + e1;
-            if (!want_grad && two && b1 != cur_b) {
+            if (!pair_atomics && !want_grad && two && b1 != cur_b) {
                 cur_b = b1;
                 cb = cb1;
             }
-            if (want_grad) {
+            if (want_grad && pair_atomics) {
+                if (in0) {
+                    const int Fx = to_fixed(g0 * r0x, fix), Fy = to_fixed(g0 * r0y, fix), Fz = to_fixed(g0 * r0z, fix);
+                    atomicAdd(&qx[a0], -Fx); atomicAdd(&qy[a0], -Fy); atomicAdd(&qz[a0], -Fz);
+                    atomicAdd(&qx[b0], Fx); atomicAdd(&qy[b0], Fy); atomicAdd(&qz[b0], Fz);
+                }
+                if (in1) {
+                    const int Fx = to_fixed(g1 * r1x, fix), Fy = to_fixed(g1 * r1y, fix), Fz = to_fixed(g1 * r1z, fix);
+                    atomicAdd(&qx[a1], -Fx); atomicAdd(&qy[a1], -Fy); atomicAdd(&qz[a1], -Fz);
+                    atomicAdd(&qx[b1], Fx); atomicAdd(&qy[b1], Fy); atomicAdd(&qz[b1], Fz);
+                }
+            } else if (want_grad) {
                 if (in0) {
                     const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
                     atomicAdd(&qx[a0], to_fixed(-Fx, fix)); atomicAdd(&qy[a0], to_fixed(-Fy, fix));
@@ -467,11 +484,11 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     return e;
 }
 
-template <bool want_grad>
+template <bool want_grad, bool pair_atomics = false>
 __device__ __forceinline__ float eval_pose(const LigView& L, const WarpMem& m, const MapView& G,
                                            const float4* smooth, const EvalParams ep, int lane) {
     const GridInter gi{&G, ep.v_inter, ep.slope};
-    return eval_pose_t<want_grad>(L, m, gi, smooth, ep.v_intra, ep.fix, ep.inv_fix, lane);
+    return eval_pose_t<want_grad, pair_atomics>(L, m, gi, smooth, ep.v_intra, ep.fix, ep.inv_fix, lane);
 }
 
 }  // namespace vd

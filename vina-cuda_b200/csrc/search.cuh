@@ -118,7 +118,7 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
                            const EvalParams ep, int max_steps, int lane, int& evals) {
     const int n = 6 + L.nt, nc = 7 + L.nt;
     if (max_steps <= 0) max_steps = 1000;  // the reference's 0 means unbounded
-    float fx = eval_pose<true>(L, s.m, G, smooth, ep, lane);
+    float fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane);
     ++evals;
     Vec2 g = vload(s.m.g, n, lane);
     const float fx_orig = fx;
@@ -145,7 +145,7 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
                 const float finit = fx, dgtest = 1.0e-4f * dginit, dstest = 0.1f * dginit;
                 for (;;) {
                     conf_step(s.xp, s.m.x, d, step, L.nt, lane);
-                    fx = eval_pose<true>(L, s.m, G, smooth, ep, lane);
+                    fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane);
                     ++evals;
                     g = vload(s.m.g, n, lane);
                     ++count;
