@@ -131,7 +131,7 @@ def lig_bytes(lig):
 # captured with this kernel.  The bench scales the figure by the evaluations
 # of each launch.
 DOCK_DRAM_BYTES_PER_EVAL = {1: 564.0, 3: 2700.0, 4: 427.0, 5: 335.0}
-DOCK_SHAPES = 5  # launch shapes the docking autotuner explores (register budgets)
+DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 
 
 def peaks():
@@ -322,7 +322,9 @@ def _uneven_line(cpu, threads):
     ctx.build_grids(synth.TYPES8)
     ids = [ctx.add_ligand(l) for l in ligs]
     per = cfg["total_chains"] // cfg["ligands"]
-    sp = vdock.search_params(seed=SEED, n_chains=per, search_depth=cfg["steps"], refine=1, launch_shape=1)
+    sp = vdock.search_params(seed=SEED, n_chains=per, search_depth=cfg["steps"], refine=1)
+    for _ in range(DOCK_SHAPES):  # untimed: the autotuner runs each of its shapes once
+        ctx.dock_batched(ids, sp)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = ctx.dock_batched(ids, sp)
@@ -331,7 +333,8 @@ def _uneven_line(cpu, threads):
     evals = sum(int(r["bfgs_evals"]) for r in res)
     line = {"s": wall, "ligands_per_s": len(ids) / wall, "dock_ms": st["dock_ms"], "post_ms": st["post_ms"],
             "bfgs_evals": evals, "bfgs_evals_per_s": evals / (st["dock_ms"] / 1e3), "chains_per_ligand": per,
-            "launch_shape": st["dock_shape"], "graph_launches": st["graph_launches"]}
+            "launch_shape": st["dock_shape"], "graph_launches": st["graph_launches"],
+            "untimed_warmup_calls": DOCK_SHAPES}
     ctx.close()
     if cpu:
         orc = oracle_lib.Oracle()

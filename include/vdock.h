@@ -89,10 +89,10 @@ typedef struct {
     double   min_rmsd;        /* cluster radius 1.0                            */
     int32_t  refine;          /* 1 = refine + rescore on the GPU (main.cpp:434)*/
     int32_t  launch_shape;    /* docking kernel shape: 0 = autotuned per
-                                 workload, 1/2/3/4/5 = 64/48/40/80/128
-                                 registers per thread (8/10/12/6/4 blocks of
-                                 4 chains per SM); results do not depend on
-                                 it                                         */
+                                 workload (among 1, 4, 5), 1/2/3/4/5 =
+                                 64/48/40/80/128 registers per thread
+                                 (8/10/12/6/4 blocks of 4 chains per SM);
+                                 results do not depend on it                */
 } vd_search_params;
 
 typedef struct {

@@ -144,13 +144,22 @@ DockFn dock_fn(int shape) {
 
 }  // namespace
 
+// The autotuner's candidates: 64, 80 and 128 registers.  The 48- and
+// 40-register shapes spill heavily and were slower on every measured
+// workload (wide-box screen, single ligand, uneven batch); they stay
+// available to callers that pin a shape.
+constexpr int kTunedShapes[] = {0, 3, 4};
+constexpr int kNumTuned = int(sizeof(kTunedShapes) / sizeof(kTunedShapes[0]));
+
 int dock_shape_for(Ctx& c, const vd_search_params& sp, uint64_t key) {
     if (sp.launch_shape >= 1 && sp.launch_shape <= kDockShapes) return sp.launch_shape - 1;
-    return c.dock_tune.pick(key, kDockShapes);
+    return kTunedShapes[c.dock_tune.pick(key, kNumTuned)];
 }
 
 void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals) {
-    if (b.tuned && evals > 0) c.dock_tune.report(b.tune_key, b.shape, ms / double(evals));
+    if (!b.tuned || evals == 0) return;
+    for (int i = 0; i < kNumTuned; ++i)
+        if (kTunedShapes[i] == b.shape) c.dock_tune.report(b.tune_key, i, ms / double(evals));
 }
 
 // Heuristics of main.cpp:354-391 for RILC-BFGS (atoms = all ligand atoms).
