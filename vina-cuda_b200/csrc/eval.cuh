@@ -8,8 +8,9 @@
 //   3. lanes = atoms: coordinates, trilinear grid term (grid.cpp:50-160)
 //   4. lanes = segments of the pair list sorted by second atom, two pairs
 //      per iteration (read from the lane-interleaved copy): intra pair term;
-//      the force on the second atom is accumulated in registers, the force
-//      on the first atom is added with a shared-memory atomic
+//      the force on the first atom is added with a shared-memory atomic, the
+//      force on the second atom either summed in registers while the atom
+//      repeats or, in the search (pair_atomics), added with an atomic too
 //      (model.cpp:1241-1256).  Pair forces are summed in 32-bit fixed point
 //      (EvalParams::fix units per kcal/mol/A, set from the tables so that
 //      no atom's sum can overflow): on B200 shared-memory 32-bit integer
@@ -24,7 +25,8 @@
 //        dE/dtorsion = T_k . axis_k (the bottom-up recursion of
 //        tree.h:169-178, 341-348, 373-422)
 //   8. warp butterfly sum of the energy (deterministic).
-// The per-body and subtree sums run in a fixed order.
+// The per-body and subtree sums run in a fixed order, so every result is
+// reproducible run to run and across launch shapes.
 #pragma once
 
 #include "checks.cuh"
