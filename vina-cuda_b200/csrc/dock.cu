@@ -58,8 +58,15 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
 // MINB: 4-warp blocks per SM the register budget targets (8/10/12/6/4 ->
 // 64/48/40/80/128 registers per thread); the autotuner picks one per
 // workload.  The small budgets keep more chains resident for large batches;
-// the large ones drop the register spills (ptxas: 188 bytes of spill stores
+// the large ones drop the register spills (ptxas: 84 bytes of spill stores
 // at 64, none at 128), which pays when a launch has few chains per SM.
+// Per-warp shared memory: the evaluation's arrays, then the poses xp, xo,
+// xt, xb (pad4(7 + ntors) floats each), then kChainWords chain scalars.
+// chain scalar slots (ints, then floats)
+enum : int { kCsItem, kCsLig, kCsChain, kCsUid, kCsDepth, kCsSteps, kCsEvals0, kCsStep, kCsFloats };
+enum : int { kCfCurrent, kCfBest };
+static_assert(kCsFloats + kCfBest + 1 <= kChainWords, "chain scalars exceed their shared words");
+
 template <bool persistent, int MINB>
 __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
     extern __shared__ float4 smem4[];
@@ -74,9 +81,8 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
             item = __shfl_sync(0xffffffffu, v, 0);
         }
         if (item >= p.total_items) break;
-        const int li = VD_DCLAMP(find_ligand(p.prefix, p.n_ligs, item), 0, p.n_ligs - 1, kChkItem);
-        const uint32_t chain = uint32_t(item - __ldg(&p.prefix[li]));
-        const LigView L = lig_view(p.pool, __ldg(&p.lig_off[li]));
+        const int li0 = VD_DCLAMP(find_ligand(p.prefix, p.n_ligs, item), 0, p.n_ligs - 1, kChkItem);
+        const LigView L = lig_view(p.pool, __ldg(&p.lig_off[li0]));
         const int nc = 7 + L.nt, nc4 = pad4(nc);
         SearchMem s;
         s.m = carve(base, L.na, L.nn, L.np, L.nt);
@@ -84,45 +90,70 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
         s.xo = s.xp + nc4;
         float* xt = s.xo + nc4;      // current (accepted) pose
         float* xb = xt + nc4;        // chain best
-        const uint32_t uid = __ldg(&p.lig_uid[li]);
-        const int depth = __ldg(&p.depth[li]), steps = __ldg(&p.bfgs_steps[li]);
-        const int evals0 = evals;
-        init_pose(xt, L.nt, p.seed, uid, chain, p.lo, p.hi, lane);
+        // The chain's scalars live in shared memory, not in registers across
+        // the optimiser calls: the evaluation needs every register it can get
+        // (at 64 registers per thread this halves the spills to local memory,
+        // whose reloads miss L1), and these are read once per MC step.
+        int* cs = reinterpret_cast<int*>(xb + nc4);
+        float* cf = reinterpret_cast<float*>(cs + kCsFloats);
+        if (lane == 0) {
+            cs[kCsItem] = item;
+            cs[kCsLig] = li0;
+            cs[kCsChain] = int(item - __ldg(&p.prefix[li0]));
+            cs[kCsUid] = int(__ldg(&p.lig_uid[li0]));
+            cs[kCsDepth] = __ldg(&p.depth[li0]);
+            cs[kCsSteps] = __ldg(&p.bfgs_steps[li0]);
+            cs[kCsEvals0] = evals;
+            cf[kCfCurrent] = FLT_MAX;
+            cf[kCfBest] = INFINITY;
+        }
+        __syncwarp();
+        init_pose(xt, L.nt, p.seed, uint32_t(cs[kCsUid]), uint32_t(cs[kCsChain]), p.lo, p.hi, lane);
         copy_conf(xt, xb, nc, lane);
-        float tmp_e = FLT_MAX, best_e = INFINITY;
-        for (int step = 0; step < depth; ++step) {
+        for (int step = 0; step < cs[kCsDepth]; ++step) {
+            if (lane == 0) cs[kCsStep] = step;
             copy_conf(xt, s.m.x, nc, lane);
-            mutate_pose(L, s.m, p.seed, uid, chain, uint32_t(step), p.amplitude, lane);
-            uint32_t b[4];
-            draw(p.seed, uid, chain, uint32_t(step), 1, b);
+            mutate_pose(L, s.m, p.seed, uint32_t(cs[kCsUid]), uint32_t(cs[kCsChain]), uint32_t(step), p.amplitude,
+                        lane);
             // pass 0 optimises the candidate; pass 1 re-optimises an accepted
             // candidate that beats the chain's best (one optimiser call site)
             for (int pass = 0; pass < 2; ++pass) {
-                const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, steps, lane, evals);
+                const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, cs[kCsSteps], lane, evals);
+                const int stp = cs[kCsStep];
+                float tmp_e = cf[kCfCurrent], best_e = cf[kCfBest];
                 if (pass == 0) {
-                    const bool accept = step == 0 || ce < tmp_e ||
+                    uint32_t b[4];
+                    draw(p.seed, uint32_t(cs[kCsUid]), uint32_t(cs[kCsChain]), uint32_t(stp), 1, b);
+                    const bool accept = stp == 0 || ce < tmp_e ||
                                         u01(b[1]) < __expf((tmp_e - ce) / p.temperature);  // kernel2.cu:63-71
                     if (!accept) break;
                     tmp_e = ce;
+                    __syncwarp();
+                    if (lane == 0) cf[kCfCurrent] = tmp_e;
                     if (!(tmp_e < best_e)) {
                         copy_conf(s.m.x, xt, nc, lane);
                         break;
                     }
                 } else {
                     tmp_e = ce;
+                    __syncwarp();
+                    if (lane == 0) cf[kCfCurrent] = tmp_e;
                     if (tmp_e < best_e) {
-                        best_e = tmp_e;
+                        if (lane == 0) cf[kCfBest] = tmp_e;
                         copy_conf(s.m.x, xb, nc, lane);
                     }
                     copy_conf(s.m.x, xt, nc, lane);
                 }
+                __syncwarp();
             }
+            step = cs[kCsStep];  // reloaded: not held in a register across the optimiser
         }
-        float* dst = p.out_conf + size_t(item) * p.stride;
+        const int it = cs[kCsItem], li = cs[kCsLig];
+        float* dst = p.out_conf + size_t(it) * p.stride;
         for (int i = lane; i < nc; i += 32) dst[i] = xb[i];
         if (lane == 0) {
-            p.out_e[item] = best_e;
-            atomicAdd(&p.lig_evals[li], (unsigned long long)(evals - evals0));
+            p.out_e[it] = cf[kCfBest];
+            atomicAdd(&p.lig_evals[li], (unsigned long long)(evals - cs[kCsEvals0]));
         }
         __syncwarp();
         if (!persistent) break;
@@ -204,7 +235,7 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
         uid[i] = uint32_t(ligs[i]);
         search_defaults(L, sp, depth[i], steps[i]);
         prefix[i + 1] = prefix[i] + sp.n_chains;
-        max_wf = std::max(max_wf, lig_warp_floats(L) + 4 * pad4(7 + L.h.ntors));
+        max_wf = std::max(max_wf, lig_warp_floats(L) + 4 * pad4(7 + L.h.ntors) + kChainWords);
         max_nt = std::max(max_nt, L.h.ntors);
     }
     const int items = prefix[n];
@@ -462,7 +493,7 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     p.queue = nullptr;  // one warp per chain: no work queue
     p.evals = d_cnt;
     p.lig_evals = d_cnt + 1;
-    p.warp_floats = lig_warp_floats(L) + 4 * pad4(nc);
+    p.warp_floats = lig_warp_floats(L) + 4 * pad4(nc) + kChainWords;
     const int wpb = 4;
     const size_t smem = size_t(p.warp_floats) * wpb * sizeof(float);
     VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "vd_mc_chains_noalloc: ligand too large for the kernel");

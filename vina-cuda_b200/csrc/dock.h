@@ -26,6 +26,7 @@ struct DockBuffers {
 };
 
 constexpr int kDockShapes = 5;      // register budgets 64/48/40/80/128 per thread
+constexpr int kChainWords = 16;     // per-warp shared words for a chain's scalars (dock_kernel)
 
 void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps);
 // prepare_dock: host work and device layout (no stream operation);
