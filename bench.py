@@ -125,12 +125,12 @@ def lig_bytes(lig):
 
 # DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
 # captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
-# ligands x 6,500 chains, 11.54 M evaluations per launch): 64 registers
-# 6.51 GB, 40 registers 31.17 GB, 80 registers 4.93 GB, 128 registers
-# 3.87 GB (the difference is register spills); the 48-register shape was not
-# captured with this kernel.  The bench scales the figure by the evaluations
-# of each launch.
-DOCK_DRAM_BYTES_PER_EVAL = {1: 564.0, 3: 2700.0, 4: 427.0, 5: 335.0}
+# ligands x 6,500 chains, 11.55 M evaluations per launch): 64 registers
+# 5.77 GB, 80 registers 4.52 GB, 128 registers 3.88 GB (the difference is
+# register spills).  The 48- and 40-register shapes, which the autotuner no
+# longer runs, were not captured with this kernel.  The bench scales the
+# figure by the evaluations of each launch.
+DOCK_DRAM_BYTES_PER_EVAL = {1: 499.0, 4: 392.0, 5: 336.0}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 
 
