@@ -205,6 +205,25 @@ def test_autotuner_logic(tmp_path):
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
 
 
+def test_pair_force_scale_host_check(tmp_path):
+    """The fixed-point scale of the kernels' pair-force sums (tables.cpp
+    pair_force_scale) for weights from 1/100 to 1000 times the defaults:
+    a power of two, the largest whose per-atom sums cannot overflow; 2^19
+    for the default weights (a compiled host check)."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "fixed_scale_check"
+    inc = os.path.join(REPO, "vina-cuda_b200", "csrc")
+    srcs = [os.path.join(REPO, "tests", "host", "fixed_scale_check.cpp"), os.path.join(inc, "tables.cpp")]
+    subprocess.run([gxx, "-std=c++17", "-O2", "-Wall", "-ffp-contract=off", "-I", inc, "-I", "/usr/local/cuda/include",
+                    *srcs, "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
+
+
 def _mutate(lines, rng):
     keys = ["ROOT", "ENDROOT", "BRANCH   1   2", "ENDBRANCH   1   2", "TORSDOF 3", "MODEL 1", "ENDMDL", "BRANCH",
             "BRANCH 9999 1", "ENDBRANCH 5 5", ""]
