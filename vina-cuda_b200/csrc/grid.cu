@@ -14,10 +14,10 @@
 // memory, the receptor atoms whose brick distance to the tile is below the
 // cutoff, taken from per-type 4 A cell lists in deterministic (receptor type,
 // cell, index) order.  The bin index floor(32 r^2) comes from a rounded-down
-// FP64 add of 2^52 (no FP64->int conversion), every point then reads one
-// 32-byte table row (a zero row beyond the cutoff, so the four loads of a
-// thread issue together) and the accumulators are packed FP32 pairs added
-// with add.rn.f32x2.
+// FP64 add of 2^52 (no FP64->int conversion), every point within the cutoff
+// then reads one 32-byte table row (predicated loads, so a thread's four
+// issue together) and the accumulators are packed FP32 pairs added with
+// add.rn.f32x2.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -31,7 +31,7 @@ namespace {
 constexpr int kTileX = 16, kTileY = 8;  // z tile (TZ = 8 or 4) is a launch shape; threads = 32 * TZ
 constexpr int kStageCap = 128;    // atoms staged per chunk (4 KB; a 70 A tile keeps ~60, larger counts loop)
 constexpr double kCellSize = 4.0;
-constexpr int kLutRows = kBins + 1;  // table rows per receptor type; the last is zero
+constexpr int kLutRows = kBins + 1;  // table rows per receptor type; the last (zero) row is padding
 
 struct StagedAtom {
     double x, y, z;
@@ -228,9 +228,10 @@ __global__ void __launch_bounds__(32 * TZ, 16 / TZ) grid_build_kernel(GridParams
                 const double dy = __dsub_rn(at.y, py), dz = __dsub_rn(at.z, pz);
                 const double dy2 = __dmul_rn(dy, dy), dz2 = __dmul_rn(dz, dz);
                 if (__dadd_rn(dy2, dz2) > kCutoff2) continue;  // exact: sums are monotone
-                // Every point loads a row; points beyond the cutoff read the
-                // type's zero row (always an L1 hit), so the four loads issue
-                // back to back instead of behind one branch each.
+                // Each point within the cutoff loads its row; the loads are
+                // predicated per point (no branch), so those of a thread still
+                // issue back to back, and points beyond the cutoff cost no L1
+                // wavefront (the kernel's limit).
                 const float* row_base = p.lut + VD_DCLAMP(at.type, 0, p.n_rtypes - 1, kChkGridType) * (kLutRows * NTG);
                 int bin[4];
 #pragma unroll
@@ -240,7 +241,8 @@ __global__ void __launch_bounds__(32 * TZ, 16 / TZ) grid_build_kernel(GridParams
                     bin[k] = r2 <= kCutoff2 ? bin_of(r2) : kBins;
                 }
 #pragma unroll
-                for (int k = 0; k < 4; ++k) add_row<NTG>(acc[k], row_base + bin[k] * NTG);
+                for (int k = 0; k < 4; ++k)
+                    if (bin[k] < kBins) add_row<NTG>(acc[k], row_base + bin[k] * NTG);
             }
         }
         if (kept <= chunk + kStageCap) break;
