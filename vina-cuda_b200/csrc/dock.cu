@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
         init_pose(xt, L.nt, p.seed, uint32_t(cs[kCsUid]), uint32_t(cs[kCsChain]), p.lo, p.hi, lane);
         copy_conf(xt, xb, nc, lane);
         for (int step = 0; step < cs[kCsDepth]; ++step) {
+            __syncwarp();  // every lane has read the previous step index
             if (lane == 0) cs[kCsStep] = step;
             copy_conf(xt, s.m.x, nc, lane);
             mutate_pose(L, s.m, p.seed, uint32_t(cs[kCsUid]), uint32_t(cs[kCsChain]), uint32_t(step), p.amplitude,
