@@ -200,17 +200,22 @@ vd_status vd_local_opt(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, float* pose
 vd_status vd_mc_chains(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,
                        float* poses_out, float* e_out, int64_t* evals);
 /* Same chains as vd_mc_chains (same kernel and random streams) for callers
- * that cannot allocate device memory when they dock -- code recording into a
- * CUDA graph, where an allocation breaks the capture, or hosts that reserve
- * their whole device budget up front.  No counterpart in the reference.
+ * that cannot allocate device memory when they dock: hosts that reserve
+ * their whole device-memory budget up front (a pool owning every free byte,
+ * a service that must not grow its footprint on a shared GPU) and
+ * latency-sensitive hosts that cannot take the device-wide synchronisation
+ * an allocation may imply.  No counterpart in the reference.
  * It allocates nothing: parameters, counters and results pass through a
- * static device array of VD_NOALLOC_SCRATCH_BYTES that every GPU loading the
- * library holds until exit; calls needing more are rejected
+ * static device array of VD_NOALLOC_SCRATCH_BYTES (4 MiB) that every GPU
+ * loading the library holds until exit; calls needing more are rejected
  * (VD_ERR_CAPACITY).  All calls on a device share that array and it keeps
  * the last call's contents, so calls whose GPU work overlaps race: serialise
  * them.  Ligands must already be on the device (one allocating call after
  * vd_add_ligand).  The first call on a device looks up the array's address
- * once; make it before any stream capture. */
+ * once (set-up); make it before any stream capture.  sp->launch_shape is not
+ * read: the kernel runs at the 64-register shape (chains are identical at
+ * every shape).  Evaluations are added to vd_stats.bfgs_evals; dock_ms is
+ * not updated. */
 #define VD_NOALLOC_SCRATCH_BYTES (4u << 20)
 vd_status vd_mc_chains_noalloc(vd_ctx* ctx, int32_t lig_id, const vd_search_params* sp,
                                float* poses_out, float* e_out, int64_t* evals);

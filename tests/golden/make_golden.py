@@ -1,8 +1,12 @@
 """Generates the golden fixtures under tests/golden/ from the reference tree.
 
-Runs only where the reference checkout exists (it reads
-/root/reference); the fixtures it writes are committed so the tests need no
-reference files at run time.
+Runs only where a checkout of the reference exists; its root (the directory
+holding Vina-CUDA_v1.1/ and QuickVina-W-CUDA/) is the one argument:
+
+    python tests/golden/make_golden.py <reference root>
+
+The fixtures it writes are committed so the tests need no reference files at
+run time.
 
 Outputs
 * kat_vina.npz -- known-answer vectors: for each docked ligand the reference
@@ -26,12 +30,11 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "oracle"))
 import pdbqt_oracle as P  # noqa: E402
 
-REF = "/root/reference"
-V11 = os.path.join(REF, "Vina-CUDA_v1.1")
-QW = os.path.join(REF, "QuickVina-W-CUDA", "input_file_example")
 
 
-def main():
+def main(ref):
+    V11 = os.path.join(ref, "Vina-CUDA_v1.1")
+    QW = os.path.join(ref, "QuickVina-W-CUDA", "input_file_example")
     cfg = P.read_config(open(os.path.join(V11, "input_file_example/1u1b_config.txt")).read())
     center = [float(cfg[k]) for k in ("center_x", "center_y", "center_z")]
     size = [float(cfg[k]) for k in ("size_x", "size_y", "size_z")]
@@ -46,7 +49,7 @@ def main():
         ligs = [P.parse_ligand(t) for _, t in models]
         d = ligs[0].descriptor()
         key = f"L{len(names)}"
-        names.append(os.path.relpath(f, REF))
+        names.append(os.path.relpath(f, ref))
         for k in ("xs", "el", "atom_node", "node_parent", "node_origin_atom", "node_axis_atom", "pairs"):
             out[f"{key}_{k}"] = d[k]
         out[f"{key}_num_tors"] = np.array(d["num_tors"])
@@ -65,10 +68,12 @@ def main():
         "1u1b_docking_result.pdbqt": os.path.join(V11, "docking_result/1u1b_docking_result.pdbqt"),
     }
     for dst, src in copies.items():
-        with open(src, "rb") as fi, gzip.open(os.path.join(HERE, "pdbqt", dst + ".gz"), "wb") as fo:
+        with open(src, "rb") as fi, gzip.GzipFile(os.path.join(HERE, "pdbqt", dst + ".gz"), "wb", mtime=0) as fo:
             fo.write(fi.read())
     print(f"wrote {len(names)} known-answer ligands")
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], "Vina-CUDA_v1.1")):
+        sys.exit("usage: make_golden.py <reference root containing Vina-CUDA_v1.1/>")
+    main(sys.argv[1])

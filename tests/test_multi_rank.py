@@ -46,6 +46,10 @@ def test_cost_matches_search_heuristics():
     c = multi.ligand_cost(24, 24, 5, 200)
     assert c == 7 * 18 * (32.0 * 24 + 16.0 * 200)
     assert multi.ligand_cost(24, 24, 5, 200, search_depth=1000, max_bfgs_steps=5) == 1000 * 5 * (32.0 * 24 + 16.0 * 200)
+    # dense BFGS (--rilc_bfgs 0): depth int((...) * 2.4) = 9, steps (25+24)//3 = 16 (main.cpp:367-389)
+    assert multi.ligand_cost(24, 24, 5, 200, dense_bfgs=True) == 9 * 16 * (32.0 * 24 + 16.0 * 200)
+    # a negative depth runs no MC step (chains return their initial poses)
+    assert multi.ligand_cost(24, 24, 5, 200, search_depth=-1) == 32.0 * 24 + 16.0 * 200
 
 
 def _worker(rank, world, port, mode, q):

@@ -387,12 +387,14 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
 // ---------------------------------------------------------------------------
 // Monte-Carlo chains without any device allocation.
 //
-// Some callers cannot call cudaMalloc at the moment they dock: code that
-// records its GPU work into a CUDA graph (an allocation inside stream capture
-// breaks the capture), and host applications that reserve their whole device
-// memory budget up front and forbid allocations afterwards.  This entry point
-// keeps its launch parameters, counters and per-chain results in one
-// statically sized device array instead of the context's growable scratch.
+// Some callers cannot call cudaMalloc at the moment they dock: host
+// applications that reserve their whole device-memory budget up front (a
+// memory pool that owns every free byte, or a service that must not grow its
+// footprint once it is admitted to a shared GPU), and latency-sensitive hosts
+// that cannot afford the device-wide synchronisation an allocation or free may
+// imply.  This entry point keeps its launch parameters, counters and
+// per-chain results in one statically sized device array instead of the
+// context's growable scratch.
 //
 // Limits and sharing: the array holds VD_NOALLOC_SCRATCH_BYTES; a call whose
 // chains do not fit is rejected with VD_ERR_CAPACITY.  Every GPU that loads
@@ -401,7 +403,9 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
 // cleared by each call), so calls whose GPU work overlaps race with each
 // other: serialise them.  The first call on a device looks up the array's
 // device address with that device current (one-time set-up); make that first
-// call before any stream capture.
+// call before any stream capture.  The kernel always runs at the 64-register
+// launch shape (sp->launch_shape is not read); chains do not depend on the
+// shape.
 namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[VD_NOALLOC_SCRATCH_BYTES];
@@ -508,6 +512,8 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     unsigned long long ev = 0;
     VD_CUDA(cudaMemcpyAsync(&ev, d_cnt, sizeof(ev), cudaMemcpyDeviceToHost, c.stream));
     VD_CUDA(cudaStreamSynchronize(c.stream));
+    if ((st = take_device_checks("vd_mc_chains_noalloc")) != VD_OK) return st;
+    c.stats.bfgs_evals += int64_t(ev);
     if (evals) *evals = int64_t(ev);
     return VD_OK;
 }

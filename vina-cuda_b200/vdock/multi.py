@@ -20,22 +20,28 @@ import heapq
 MAX_TORS = 48
 
 
-def ligand_cost(n_atoms, n_heavy, ntors, n_pairs, search_depth=0, max_bfgs_steps=0):
+def ligand_cost(n_atoms, n_heavy, ntors, n_pairs, search_depth=0, max_bfgs_steps=0, dense_bfgs=False):
     """Relative cost of docking one ligand: MC steps x BFGS steps x bytes per
-    evaluation (main.cpp:369-386 heuristics when the depth / steps are 0)."""
+    evaluation, with the heuristics of main.cpp:367-389 when the depth / steps
+    are 0 (x2 and (30 + atoms)/3 for RILC-BFGS, x2.4 and (25 + atoms)/3 for
+    dense BFGS) and, as the docking kernel does, no MC steps for a negative
+    depth (each chain returns its initial pose: one evaluation's bytes)."""
+    per_eval = 32.0 * n_heavy + 16.0 * n_pairs
+    if search_depth < 0:
+        return per_eval
     depth = search_depth
     if depth == 0:
-        depth = max(1, int((0.24 * n_atoms + 0.29 * ntors - 3.41) * 2))
-    depth = max(depth, 1)
-    steps = max_bfgs_steps if max_bfgs_steps > 0 else (30 + n_atoms) // 3
-    return float(depth) * steps * (32.0 * n_heavy + 16.0 * n_pairs)
+        depth = max(1, int((0.24 * n_atoms + 0.29 * ntors - 3.41) * (2.4 if dense_bfgs else 2.0)))
+    steps = max_bfgs_steps if max_bfgs_steps > 0 else ((25 if dense_bfgs else 30) + n_atoms) // 3
+    return float(depth) * steps * per_eval
 
 
-def desc_cost(lig, search_depth=0, max_bfgs_steps=0):
+def desc_cost(lig, search_depth=0, max_bfgs_steps=0, dense_bfgs=False):
     """ligand_cost of a ligand description dict (vdock.synth / PDBQT form)."""
     n_heavy = int(sum(1 for t in lig["xs"] if t >= 0))
     ntors = len(lig["node_parent"]) - 1
-    return ligand_cost(int(lig["n_atoms"]), n_heavy, ntors, len(lig["pairs"]), search_depth, max_bfgs_steps)
+    return ligand_cost(int(lig["n_atoms"]), n_heavy, ntors, len(lig["pairs"]), search_depth, max_bfgs_steps,
+                       dense_bfgs)
 
 
 def shard_by_cost(costs, world):
