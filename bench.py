@@ -9,7 +9,8 @@ each docked with 6,500 Monte-Carlo chains (RILC-BFGS local search, heuristic
 search depth) followed by GPU clustering, refinement and rescoring of its
 top 20 poses.  One step = one batch of ligands through vd_dock_batched (one
 persistent launch over all (ligand, chain) items).  The plain form
-(vd_dock_plain, one ligand per launch) is timed on a sample beside it.
+(vd_dock_plain, one ligand per launch) is timed beside it on the ligands of
+the first timed batch.
 
 Run: python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 Under torchrun each rank docks its own ligand batches (weak scaling, no
@@ -44,7 +45,6 @@ def args_():
     a.add_argument("--impl", default="ours", choices=["ours", "reference"])
     a.add_argument("--batch", type=int, default=64, help="ligands per step")
     a.add_argument("--chains", type=int, default=CHAINS)
-    a.add_argument("--plain-ligands", type=int, default=8)
     a.add_argument("--e2e-steps", type=int, default=0,
                    help="timed batches re-run end to end (0 = all K, the same batches as the timed region)")
     a.add_argument("--no-cpu-baseline", action="store_true")
@@ -387,12 +387,17 @@ def run_reference(a):
     sample = (f"{a.steps} steps x {n} whole ligands ({'; '.join(descs)}), {a.chains} chains each, heuristic "
               f"depth, top-20 refinement; {evals:.0f} BFGS evals in {total_t:.1f} s (after {a.warmup} warm-up steps)")
     threads = os.cpu_count() or 1
+    # ms_per_step: the measured time of one step's sample (a.cpu_ligands whole
+    # ligands), not an extrapolation to the GPU arm's batch
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": 1e3 * a.batch / value, "higher_is_better": True,
+            "warmup": a.warmup, "ms_per_step": 1e3 * total_t / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "wide-box screen", "ligands_per_step": a.batch, "chains_per_ligand": a.chains,
-                       "box_A": BOX, "receptor_atoms": REC_ATOMS},
+            "config": {"workload": "wide-box screen", "ligands_per_step": a.batch,
+                       "ligands_timed_per_step": n, "chains_per_ligand": a.chains,
+                       "search_depth": "heuristic (main.cpp:369)", "box_A": BOX, "receptor_atoms": REC_ATOMS,
+                       "ligand_atoms": list(LIG_ATOMS), "ligand_torsions": list(LIG_TORS),
+                       "parallelism": "host threads (oracle port)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "grid_build_s": t_grid,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -414,7 +419,7 @@ def run_ours(a):
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = td
     B, W, K = a.batch, a.warmup, a.steps
-    n_ligs = (W + K) * B + a.plain_ligands
+    n_ligs = (W + K) * B
     xyz, xs, ligs = make_inputs(rank, n_ligs)
     ctx = vdock.Context(local)
     ctx.set_receptor(xyz, xs)
@@ -441,13 +446,14 @@ def run_ours(a):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record()
-    dock_ms, evals, abytes, launches = 0.0, 0, 0, 0
+    dock_ms, post_ms, evals, abytes, launches = 0.0, 0.0, 0, 0, 0
     t_wall = time.perf_counter()
     for k in range(W, W + K):
         res = ctx.dock_batched(batches[k], sp)
         st = ctx.stats()
         shapes = {"dock_launch_shape": st["dock_shape"], "grid_shape": st["grid_shape"]}
         dock_ms += st["dock_ms"]
+        post_ms += st["post_ms"]
         for lid, r in zip(batches[k], res):
             evals += r["bfgs_evals"]
             abytes += r["bfgs_evals"] * lig_bytes(ligs[lid])
@@ -462,16 +468,41 @@ def run_ours(a):
         elapsed = multi.max_over_ranks(elapsed, device="cuda")
         pg.barrier()
     value = K * B * world / elapsed
-    # plain form on a sample (one ligand per launch)
-    plain_ids = ids[(W + K) * B:]
+    # plain form, like for like: one ligand per launch (vd_dock_plain) over the
+    # same ligands, seed and chains as the first timed batch; per ligand the
+    # docking kernel's time, the post-processing kernels' time and the rest
+    # (host work, uploads, launch and synchronisation gaps), beside the same
+    # split of the batched steps
     for i in range(DOCK_SHAPES):  # warm-up: the autotuner tries each launch shape
         ctx.dock_plain(batches[0][i % len(batches[0])], sp)
     torch.cuda.synchronize()
+    p_dock = p_post = 0.0
+    p_evals, p_shapes, p_blocks = 0, set(), 0
     t0 = time.perf_counter()
-    for lid in plain_ids:
-        ctx.dock_plain(lid, sp)
+    for lid in batches[W]:
+        r = ctx.dock_plain(lid, sp)
+        st = ctx.stats()
+        p_dock += st["dock_ms"]
+        p_post += st["post_ms"]
+        p_evals += r["bfgs_evals"]
+        p_shapes.add(st["dock_shape"])
+        p_blocks = st["dock_blocks"]
     torch.cuda.synchronize()
-    plain_value = len(plain_ids) / (time.perf_counter() - t0)
+    p_wall = time.perf_counter() - t0
+    plain_value = B / p_wall
+    blocks_per_sm = {1: 8, 2: 10, 3: 12, 4: 6, 5: 4}  # four-chain blocks per SM of each register budget
+    n_sm = torch.cuda.get_device_properties(local).multi_processor_count
+    plain_split = {
+        "ligands": B, "same_ligands_as": "timed step 1", "wall_ms_per_ligand": 1e3 * p_wall / B,
+        "dock_kernel_ms_per_ligand": p_dock / B, "post_kernels_ms_per_ligand": p_post / B,
+        "host_and_gaps_ms_per_ligand": 1e3 * p_wall / B - (p_dock + p_post) / B,
+        "dock_kernel_evals_per_s": p_evals / (p_dock / 1e3), "launch_shapes": sorted(p_shapes),
+        "dock_waves": [p_blocks / (n_sm * blocks_per_sm[s]) for s in sorted(p_shapes)]}
+    batched_split = {
+        "wall_ms_per_ligand": 1e3 * elapsed / (K * B), "dock_kernel_ms_per_ligand": dock_ms / (K * B),
+        "post_kernels_ms_per_ligand": post_ms / (K * B),
+        "host_and_gaps_ms_per_ligand": 1e3 * elapsed / (K * B) - (dock_ms + post_ms) / (K * B),
+        "dock_kernel_evals_per_s": evals / (dock_ms / 1e3)}
     # end to end through the public API with host buffers: ligand topologies
     # copied in (vd_add_ligand + pool upload), results read back
     e2e_times, h2d, d2h = [], 0, 0
@@ -509,8 +540,9 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (8 maps x 188^3 x 4 B = 213 MB)",
                    "untimed_warmup_calls": n_warm, **shapes},
         "bfgs_evals_per_s": evals * world / elapsed,
-        "plain": {"value": plain_value * world, "unit": UNIT, "ligands": len(plain_ids),
-                  "batched_over_plain": value / (plain_value * world)},
+        "plain": {"value": plain_value * world, "unit": UNIT, "batched_over_plain": value / (plain_value * world),
+                  **plain_split},
+        "batched_split": batched_split,
         "grid_build": {"ms": min(grid_ms), "points": n_pts, "types": 8,
                        "gbs": grid_bytes / (min(grid_ms) / 1e3) / 1e9,
                        "frac_of_hbm": grid_bytes / (min(grid_ms) / 1e3) / 1e9 / hbm},

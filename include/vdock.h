@@ -81,6 +81,7 @@ typedef struct {
     int32_t  search_depth;    /* MC steps per chain; 0 = main.cpp:354-391 rule,
                                  < 0 = none (chains return their initial pose) */
     int32_t  max_bfgs_steps;  /* 0 = (30 + atoms)/3 (main.cpp:386)             */
+                              /* (25 + atoms)/3 with dense_bfgs             */
     int32_t  num_modes;       /* modes returned (<= VD_MAX_MODES)              */
     double   energy_range;    /* kcal/mol window above the best mode           */
     double   hunt_cap[3];     /* (10,10,10), main.cpp:395                      */
@@ -93,6 +94,12 @@ typedef struct {
                                  64/48/40/80/128 registers per thread
                                  (8/10/12/6/4 blocks of 4 chains per SM);
                                  results do not depend on it                */
+    int32_t  dense_bfgs;      /* local search of the Monte-Carlo steps:
+                                 0 = RILC-BFGS (--rilc_bfgs 1, default,
+                                 quasi_newton.cuh:2172-2389); 1 = dense BFGS
+                                 (--rilc_bfgs 0, kernel2.cu:427-563): heuristic
+                                 depth x 2.4 and (25 + atoms)/3 steps,
+                                 main.cpp:367-389                           */
 } vd_search_params;
 
 typedef struct {
@@ -124,6 +131,10 @@ typedef struct {
     double  pair_force_scale;    /* fixed-point units per kcal/mol/A in which the
                                     kernels sum intra-pair forces (a power of two
                                     set from the current tables; 2^19 by default) */
+    double  cells_ms;            /* last vd_build_grids: time to lay the maps out as
+                                    32-byte trilinear corner cells for the
+                                    evaluation kernels (0 when the box is too
+                                    large for them and the kernels read the maps) */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */
@@ -236,6 +247,12 @@ vd_status vd_refine(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, float* poses,
  * reference, plus the intramolecular energies themselves. */
 vd_status vd_score(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
                    float* adjusted_out, float* intra_out);
+
+/* RMSD lower / upper bounds of each pose's heavy atoms to pose 0
+ * (model.cpp:1485-1523, the rmsd l.b. / u.b. of the REMARK VINA RESULT lines,
+ * main.cpp:159-170); the same device code as vd_dock_*'s mode output. */
+vd_status vd_rmsd_bounds(vd_ctx* ctx, int32_t lig_id, int32_t n_poses, const float* poses,
+                         float* lb_out, float* ub_out);
 
 /* ---- host helpers (no GPU work) --------------------------------------------- */
 /* Pair tables built by vd_set_scoring: fast[153][2051], smooth e / dor. */

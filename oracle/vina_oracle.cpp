@@ -889,9 +889,39 @@ void mutate(const Lig& L, double* x, uint32_t seed, uint32_t lig, uint32_t chain
     x[7 + which - 2] = -kPi + 2 * kPi * u01(b.u[0]);
 }
 
-// kernel2.cu:219-426: MC chain with RILC-BFGS local search.
+// kernel2.cu:219-426: MC chain with RILC-BFGS local search; with s.dense,
+// kernel2.cu:427-563: dense BFGS (bfgs_optimized, quasi_newton.cuh:2391-2499)
+// and no effective re-optimisation of an accepted pose that beats the best:
+// that branch re-optimises a copy (`candidate`) and then keeps `tmp`, whose
+// energy it did not change (kernel2.cu:526-552), so the best pose and energy
+// are the accepted candidate's.
 double mc_chain(const or_ctx* c, const Lig& L, const or_search& s, uint32_t chain, double* best,
                 int64_t& evals) {
+    if (s.dense) {
+        const int nc = 7 + L.ntors();
+        Objective obj{c, &L, s.hunt_cap, s.slope, eval_deriv_cache};
+        std::vector<double> tmp(nc), cand(nc);
+        init_conf(c, L, s.seed, s.lig_uid, chain, tmp.data());
+        double tmp_e = kMax, best_e = std::numeric_limits<double>::infinity();
+        std::memcpy(best, tmp.data(), sizeof(double) * nc);
+        for (int step = 0; step < s.search_depth; ++step) {
+            cand = tmp;
+            mutate(L, cand.data(), s.seed, s.lig_uid, chain, uint32_t(step), s.amplitude, obj.F);
+            const double ce = dense_bfgs(obj, L.ntors(), cand.data(), s.max_bfgs_steps);
+            Draw b(s.seed, s.lig_uid, chain, uint32_t(step), 1);
+            const bool acc = step == 0 || ce < tmp_e || u01(b.u[1]) < std::exp((tmp_e - ce) / s.temperature);
+            if (acc) {
+                tmp = cand;
+                tmp_e = ce;
+                if (tmp_e < best_e) {
+                    best_e = tmp_e;
+                    std::memcpy(best, tmp.data(), sizeof(double) * nc);
+                }
+            }
+        }
+        evals += obj.evals;
+        return best_e;
+    }
     const int nc = 7 + L.ntors();
     Objective obj{c, &L, s.hunt_cap, s.slope, eval_deriv_cache};
     std::vector<double> tmp(nc), cand(nc);

@@ -90,10 +90,13 @@ typedef struct {
     double   slope;          /* 1e6                                         */
     double   temperature;    /* 1.2                                         */
     double   amplitude;      /* 2                                           */
+    int32_t  dense;          /* 0: RILC-BFGS local search (--rilc_bfgs 1);
+                                1: dense BFGS (--rilc_bfgs 0)               */
 } or_search;
 
 /* Runs chains [chain_begin, chain_end) of the Monte-Carlo search
- * (kernel2.cu:219-426 semantics, Philox streams shared with the GPU code).
+ * (kernel2.cu:219-426 semantics for RILC-BFGS, 427-563 for dense BFGS;
+ * Philox streams shared with the GPU code).
  * out_conf: [n*(7+ntors)], out_e: [n]; threads: host threads to use. */
 int64_t or_mc_chains(or_ctx*, int lig, const or_search*, int chain_begin, int chain_end,
                      double* out_conf, double* out_e, int threads);

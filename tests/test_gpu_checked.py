@@ -5,10 +5,15 @@ also built with -DVD_CHECKS: every device index that host validation is meant
 to keep in range (intra-pair atoms, type pairs, table bins, body parents,
 work items, grid rows and staged types, kept chains, receptor cells) is
 tested in the kernel, clamped into range when it is not, and the call fails
-with VD_ERR_CUDA naming the check.  These tests run the parity, limit and
-table suites against that library in a subprocess (VDOCK_LIB), so a silent
-out-of-range access anywhere on those paths fails them, and check that the
-checked build docks bit-identically to the normal one.
+with VD_ERR_CUDA naming the check.  These tests run the parity, limit,
+table, tuning and allocation-free suites against that library in a
+subprocess (VDOCK_LIB), and the CLI suite (single ligand with both local
+searches, and --ligand_directory batches) with the CLI linked against it
+(vdock_cli_checked, VDOCK_CLI), so a silent out-of-range access anywhere on
+those paths fails them; and they check that the checked build docks
+bit-identically to the normal one (grid maps, an uneven batched call of
+ligands with 12-60 atoms and 0-14 torsions with RILC-BFGS and with dense
+BFGS, the plain form, energies and gradients).
 """
 import os
 import subprocess
@@ -23,6 +28,7 @@ pytestmark = pytest.mark.gpu
 
 PKG = os.path.join(REPO, "vina-cuda_b200")
 CHECKED = os.path.join(PKG, "libvdock_checked.so")
+CHECKED_CLI = os.path.join(PKG, "vdock_cli_checked")
 NORMAL = os.path.join(PKG, "libvdock.so")
 
 CASE = r"""
@@ -47,15 +53,20 @@ for i, r in enumerate(ctx.dock_batched(ids, sp)):
     out[f"be{i}"], out[f"bp{i}"] = r["energy"], r["pose"]
 r = ctx.dock_plain(ids[2], sp)
 out["pe"], out["pp"] = r["energy"], r["pose"]
+spd = vdock.search_params(seed=6, n_chains=256, search_depth=2, max_bfgs_steps=8, dense_bfgs=1)
+for i, r in enumerate(ctx.dock_batched(ids, spd)):
+    out[f"de{i}"], out[f"dp{i}"] = r["energy"], r["pose"]
 poses = synth.random_poses(64, ctx.ntors[ids[3]], -6.0, 6.0, seed=3)
 out["e"], out["g"] = ctx.energy_grad(ids[3], poses)
 np.savez(sys.argv[1], **out)
 """
 
 
-def _env(lib):
+def _env(lib, cli=None):
     env = dict(os.environ)
     env["VDOCK_LIB"] = lib
+    if cli:
+        env["VDOCK_CLI"] = cli
     env["PYTHONPATH"] = os.pathsep.join([PKG, os.path.join(REPO, "oracle"), env.get("PYTHONPATH", "")])
     return env
 
@@ -69,10 +80,13 @@ def checked():
 
 
 def test_checked_build_passes_parity_limits_and_tables(checked):
+    assert os.path.exists(CHECKED_CLI), "vdock_cli_checked not built (make -C vina-cuda_b200 checked)"
     suites = [os.path.join(REPO, "tests", f) for f in
-              ("test_gpu_parity.py", "test_gpu_limits.py", "test_gpu_tables.py")]
+              ("test_gpu_parity.py", "test_gpu_limits.py", "test_gpu_tables.py", "test_gpu_tuning.py",
+               "test_gpu_cli.py", "test_zz_no_alloc.py")]
     r = subprocess.run([sys.executable, "-m", "pytest", "-x", "-q", "-m", "gpu", "-p", "no:cacheprovider",
-                        *suites], cwd=REPO, env=_env(checked), capture_output=True, text=True, timeout=1800)
+                        *suites], cwd=REPO, env=_env(checked, CHECKED_CLI), capture_output=True, text=True,
+                       timeout=2400)
     assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-2000:]
     assert " passed" in r.stdout and "skipped" not in r.stdout.split("\n")[-2], r.stdout[-800:]
 

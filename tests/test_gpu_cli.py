@@ -13,11 +13,17 @@ from conftest import REPO, has_gpu
 
 pytestmark = pytest.mark.gpu
 
+# VDOCK_CLI: another build of the CLI (the bounds-checked one, vdock_cli_checked)
+CLI = os.environ.get("VDOCK_CLI") or os.path.join(REPO, "vina-cuda_b200", "vdock_cli")
 
-def test_cli_docks_reference_example(tmp_path, golden_dir):
+
+@pytest.mark.parametrize("rilc_bfgs", [1, 0])
+def test_cli_docks_reference_example(tmp_path, golden_dir, rilc_bfgs):
+    """Both local searches of the reference's --rilc_bfgs option (main.cpp:663):
+    1 = RILC-BFGS, 0 = dense BFGS with its own depth and step heuristics."""
     if not has_gpu():
         pytest.skip("needs a CUDA device")
-    cli = os.path.join(REPO, "vina-cuda_b200", "vdock_cli")
+    cli = CLI
     assert os.path.exists(cli), "build with make -C vina-cuda_b200"
     for name in ("1u1b_protein.pdbqt", "1u1b_ligand.pdbqt", "1u1b_config.txt"):
         data = gzip.open(os.path.join(golden_dir, "pdbqt", name + ".gz"), "rb").read()
@@ -25,10 +31,11 @@ def test_cli_docks_reference_example(tmp_path, golden_dir):
     cfg = (tmp_path / "1u1b_config.txt").read_text()
     lines = [l for l in cfg.splitlines() if not l.strip().startswith(("receptor", "ligand", "out", "thread"))]
     lines += ["receptor = 1u1b_protein.pdbqt", "ligand = 1u1b_ligand.pdbqt", "out = out.pdbqt", "thread = 8192",
-              "seed = 7"]
+              "seed = 7", f"rilc_bfgs = {rilc_bfgs}"]
     (tmp_path / "cfg.txt").write_text("\n".join(lines) + "\n")
     r = subprocess.run([cli, "--config", "cfg.txt"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
+    assert "WARNING" not in r.stderr
     out = (tmp_path / "out.pdbqt").read_text()
     remarks = [l for l in out.splitlines() if l.startswith("REMARK VINA RESULT:")]
     assert 1 <= len(remarks) <= 9 and out.count("MODEL") == len(remarks) and out.count("ENDMDL") == len(remarks)
@@ -44,7 +51,7 @@ def test_cli_ligand_directory(tmp_path, golden_dir):
     message, results independent of parse timing (two runs are identical)."""
     if not has_gpu():
         pytest.skip("needs a CUDA device")
-    cli = os.path.join(REPO, "vina-cuda_b200", "vdock_cli")
+    cli = CLI
     for name in ("1u1b_protein.pdbqt", "1u1b_config.txt"):
         data = gzip.open(os.path.join(golden_dir, "pdbqt", name + ".gz"), "rb").read()
         (tmp_path / name).write_bytes(data)

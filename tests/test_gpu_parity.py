@@ -9,6 +9,8 @@ Tolerances (written here, used below):
               on a 1e5 kcal/mol energy
 * gradients:  |gpu - oracle|_inf <= 1e-3 * max(1, |oracle|_inf)
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -20,6 +22,7 @@ pytestmark = pytest.mark.gpu
 GRID_TOL = 1e-5
 E_TOL = 1e-3
 G_TOL = 1e-3
+O_THREADS = os.cpu_count() or 1
 
 
 @pytest.fixture(scope="module")
@@ -164,22 +167,68 @@ def test_mc_initial_poses_share_streams_with_oracle(vd):
         np.testing.assert_allclose(p_gpu[ch], ref, atol=2e-5)
 
 
-def test_mc_chains_match_oracle_distribution(vd):
+def _chain_stats(e_gpu, e_ref):
+    """Paired and two-sample statistics of best-of-chain energies.  se_median
+    is the standard error of the difference of the two medians from their
+    interquartile ranges (normal approximation, IQR / 1.349 per sigma), robust
+    to the out-of-box chains whose energies reach 1e6-1e8."""
+    from scipy.stats import ks_2samp, wilcoxon
+    d = e_gpu - e_ref
+    iqr = lambda v: float(np.subtract(*np.percentile(v, [75, 25])))
+    se = 1.2533 / np.sqrt(len(d)) * np.hypot(iqr(e_gpu), iqr(e_ref)) / 1.349
+    return dict(n=len(d), paired_median=float(np.median(d)), median_gpu=float(np.median(e_gpu)),
+                median_ref=float(np.median(e_ref)), ks_p=float(ks_2samp(e_gpu, e_ref).pvalue),
+                wilcoxon_p=float(wilcoxon(d).pvalue), se_median=float(se))
+
+
+@pytest.mark.parametrize("dense", [False, True], ids=["rilc", "dense"])
+def test_mc_chains_match_oracle_distribution(vd, dense):
     """Best-of-chain energies of the GPU search and of the oracle's double
-    restatement of the same search (kernel2.cu:219-426) with the same seeds:
-    each returned energy is its pose's energy, paired median difference
-    <= 0.15 kcal/mol and two-sample KS p >= 0.01."""
-    from scipy.stats import ks_2samp
+    restatement of the same search on the same Philox streams, 1,024 chains:
+    RILC-BFGS (kernel2.cu:219-426) and dense BFGS (--rilc_bfgs 0,
+    kernel2.cu:427-563).  Each returned energy is its pose's energy.
+
+    RILC-BFGS chains stay paired with the oracle's (same starts and moves;
+    FP32 and FP64 rarely take different line-search paths): the paired median
+    difference is within 0.05 kcal/mol.  Dense-BFGS chains decorrelate: with
+    the reference's identity start of the inverse Hessian a chain that starts
+    outside the box takes first steps of ~1e6 A along the 1e6 kcal/mol/A
+    penalty gradient, Armijo backtracking ends far outside, and FP32 and
+    FP64 part ways; such chains keep energies above 1e5.  So dense chains
+    are compared as distributions: the fraction of chains left outside the
+    box (Fisher's exact test p >= 0.01), and over the chains inside it the
+    difference of the medians within three of its standard errors
+    (IQR-based) and a two-sample KS test.  Both searches: two-sample KS
+    p >= 0.01 and evaluation counts within 5%."""
     ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=20, n_tors=4, seed=17, box=16.0)
-    sp = vd.search_params(seed=42, n_chains=192, search_depth=4, max_bfgs_steps=15)
+    n = 1024
+    sp = vd.search_params(seed=42, n_chains=n, search_depth=4, max_bfgs_steps=15, dense_bfgs=int(dense))
     p_gpu, e_gpu, ev = ctx.mc_chains(lc, sp)
     assert ev > 0 and np.all(np.isfinite(e_gpu))
-    conf, e_ref, _ = orc.mc_chains(lo, 42, lc, 4, 15, 0, 192, threads=8)
-    for i in range(0, 192, 16):
+    conf, e_ref, ev_ref = orc.mc_chains(lo, 42, lc, 4, 15, 0, n, threads=O_THREADS, dense=dense)
+    for i in range(0, n, 64):
         g_e, _ = orc.eval_deriv(lo, p_gpu[i].astype(np.float64))
         assert abs(g_e - e_gpu[i]) <= 1e-3 + 1e-6 * abs(g_e)
-    assert abs(np.median(e_gpu - e_ref)) <= 0.15, np.median(e_gpu - e_ref)
-    assert ks_2samp(e_gpu, e_ref).pvalue >= 0.01
+    st = _chain_stats(e_gpu, e_ref)
+    print(f"mc chains dense={dense}: {st}, evals gpu {ev} oracle {ev_ref}")
+    if dense:
+        from scipy.stats import fisher_exact, ks_2samp
+        og, orf = e_gpu > 1e5, e_ref > 1e5
+        p_out = fisher_exact([[og.sum(), n - og.sum()], [orf.sum(), n - orf.sum()]])[1]
+        eg, er = e_gpu[~og], e_ref[~orf]
+        iqr = lambda v: float(np.subtract(*np.percentile(v, [75, 25])))
+        se = 1.2533 * np.hypot(iqr(eg) / np.sqrt(len(eg)), iqr(er) / np.sqrt(len(er))) / 1.349
+        dmed = float(np.median(eg) - np.median(er))
+        print(f"dense: outside the box {int(og.sum())} / {int(orf.sum())} of {n} (Fisher p {p_out:.3g}); "
+              f"inside: medians {np.median(eg):.3f} / {np.median(er):.3f}, difference {dmed:.3f}, se {se:.3f}, "
+              f"KS p {ks_2samp(eg, er).pvalue:.3g}")
+        assert p_out >= 0.01, (og.sum(), orf.sum())
+        assert abs(dmed) <= 3 * se, (dmed, se)
+        assert ks_2samp(eg, er).pvalue >= 0.01
+    else:
+        assert abs(st["paired_median"]) <= 0.05, st
+        assert st["ks_p"] >= 0.01, st
+    assert abs(ev - ev_ref) <= 0.05 * ev_ref, (ev, ev_ref)
 
 
 def test_plain_and_batched_forms_compute_identical_chains(vd):
@@ -244,7 +293,7 @@ def test_docking_pipeline_matches_oracle_pipeline(vd):
     e = r["energy"]
     assert 1 <= len(e) <= 9 and np.all(np.diff(e) >= -1e-6) and e[-1] - e[0] <= 3.0 + 1e-6
     assert np.all(r["rmsd_ub"][1:] >= 1.0 - 1e-4) and r["rmsd_lb"][0] == 0.0
-    conf, ec, _ = orc.mc_chains(lo, 5, lc, 6, 15, 0, 512, threads=8)
+    conf, ec, _ = orc.mc_chains(lo, 5, lc, 6, 15, 0, 512, threads=O_THREADS)
     kept = orc.cluster(lo, conf, ec, 1.0, 20)
     refined = []
     for i in kept:
@@ -261,46 +310,46 @@ def test_docking_pipeline_matches_oracle_pipeline(vd):
 
 
 def test_pipeline_score_and_pose_distributions_over_seeds(vd):
-    """Best final score and top pose of the plain docking pipeline over 8
-    seeds, GPU against the oracle's restatement of the same pipeline (the
-    two take different FP paths, so runs are compared as distributions):
-    paired best scores within 0.6 kcal/mol in median and medians within
-    0.3 kcal/mol; the top poses' heavy-atom RMSD to the best pose found by
-    either (the run-to-run spread of the search) has the same distribution:
-    two-sample KS p >= 0.01, and the counts of runs that found the best
-    site (within 2 A) agree by Fisher's exact test (p >= 0.01) -- the RMSDs
-    are bimodal (the best site, or another site ~10 A away in this box), so
-    medians of 8 runs are not a usable statistic."""
+    """Best final score and top pose of the plain docking pipeline on the
+    plain-docking configuration's shapes (24-atom / 5-torsion ligand,
+    2,000-atom receptor in a 40 A ball, 20 A box, 1,024 chains, heuristic
+    search depth and BFGS steps) over 32 seeds, GPU against the oracle's
+    restatement of the same pipeline on the same seeds.  The two take
+    different floating-point paths, so runs are compared as distributions:
+    best scores by the difference of medians and a two-sample KS test, the
+    top poses by their heavy-atom RMSD to the best pose found by either (the
+    run-to-run spread of the search): KS test, and Fisher's exact test on the
+    number of runs that reach the best site (within 2 A)."""
     from scipy.stats import fisher_exact, ks_2samp
-    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=20, n_tors=4, seed=31, box=20.0, radius=40.0)
+    from pipeline_ref import heuristics, oracle_dock, top_pose_rmsd
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=24, n_tors=5, seed=31, box=20.0, radius=40.0)
+    depth, steps = heuristics(lig["n_atoms"], ctx.ntors[lc])
+    seeds = range(1, 33)
     gpu, ref = [], []
-    for seed in range(1, 9):
-        sp = vd.search_params(seed=seed, n_chains=512, search_depth=6, max_bfgs_steps=15, num_modes=9)
-        r = ctx.dock_plain(lc, sp)
+    for seed in seeds:
+        r = ctx.dock_plain(lc, vd.search_params(seed=seed, n_chains=1024, search_depth=0, num_modes=9))
         gpu.append((float(r["energy"][0]), r["pose"][0].astype(np.float64)))
-        conf, ec, _ = orc.mc_chains(lo, seed, lc, 6, 15, 0, 512, threads=8)
-        refined = []
-        for i in orc.cluster(lo, conf, ec, 1.0, 20):
-            er, c, _ = orc.refine(lo, conf[i], 15)
-            if er < 1e30:
-                refined.append((er, c))
-        refined.sort(key=lambda t: t[0])
-        ib = orc.intramolecular(lo, refined[0][1])
-        scored = sorted(((orc.eval_adjusted(lo, c, ib), c) for _, c in refined), key=lambda t: t[0])
-        ref.append(scored[0])
+        ref.append(oracle_dock(orc, lo, lc, seed, depth, steps, 1024)[0])
     eg = np.array([g[0] for g in gpu])
     er = np.array([r[0] for r in ref])
-    assert np.median(np.abs(eg - er)) <= 0.6, (eg, er)
-    assert abs(np.median(eg) - np.median(er)) <= 0.3, (eg, er)
     na = lig["n_atoms"]
     allp = [g[1] for g in gpu] + [r[1] for r in ref]
     best = allp[int(np.argmin(np.concatenate([eg, er])))]
-    xb = orc.coords(lo, best, na).ravel()
-    rg = np.array([orc.rmsd(lo, orc.coords(lo, p, na).ravel(), xb)[1] for p in allp[:8]])
-    rr = np.array([orc.rmsd(lo, orc.coords(lo, p, na).ravel(), xb)[1] for p in allp[8:]])
-    assert ks_2samp(rg, rr).pvalue >= 0.01, (rg, rr)
+    rg = np.array([top_pose_rmsd(orc, lo, na, p, best) for p in allp[:len(eg)]])
+    rr = np.array([top_pose_rmsd(orc, lo, na, p, best) for p in allp[len(eg):]])
+    n = len(eg)
     hit_g, hit_r = int((rg < 2.0).sum()), int((rr < 2.0).sum())
-    assert fisher_exact([[hit_g, 8 - hit_g], [hit_r, 8 - hit_r]])[1] >= 0.01, (rg, rr)
+    print(f"C0 seeds: depth {depth} steps {steps}; best scores gpu median {np.median(eg):.3f} sd {eg.std():.3f} "
+          f"oracle median {np.median(er):.3f} sd {er.std():.3f}; paired |d| median {np.median(np.abs(eg - er)):.3f}; "
+          f"KS p {ks_2samp(eg, er).pvalue:.3g}; rmsd KS p {ks_2samp(rg, rr).pvalue:.3g}; hits {hit_g}/{hit_r} of {n}")
+    print("gpu", np.round(eg, 2).tolist(), "\noracle", np.round(er, 2).tolist())
+    print("rmsd gpu", np.round(rg, 2).tolist(), "\nrmsd oracle", np.round(rr, 2).tolist())
+    # best scores spread by ~0.08 kcal/mol over seeds: the medians of 32 runs
+    # differ by ~0.02 kcal/mol in standard error, so 0.1 is about four of them
+    assert abs(np.median(eg) - np.median(er)) <= 0.1, (eg, er)
+    assert ks_2samp(eg, er).pvalue >= 0.01, (eg, er)
+    assert ks_2samp(rg, rr).pvalue >= 0.01, (rg, rr)
+    assert fisher_exact([[hit_g, n - hit_g], [hit_r, n - hit_r]])[1] >= 0.01, (rg, rr)
 
 
 def test_abi_rejects_malformed_inputs(vd):

@@ -235,3 +235,25 @@ def test_default_pair_forces_fit_the_fixed_point_range():
         k -= 1
     assert k == 19
     assert 127 * bound * 2.0 ** k < 2.0 ** 31
+
+
+def test_fitted_poses_reproduce_reference_remarks():
+    """The poses fitted to the reference's docked models (tests/kat_fit.py;
+    used to rescore those models through the GPU's pose-based entry points)
+    reproduce the models' coordinates to 0.005 A and, rescored by the oracle
+    from the poses, the REMARK VINA RESULT triples within the tolerances of
+    test_known_answers_all_modes (0.08 kcal/mol, 0.0015 A)."""
+    import kat_fit
+    z, o, sets = kat_fit.fitted_set()
+    n = 0
+    for i, (d, confs, remarks, fit, lid) in enumerate(sets):
+        assert fit <= 0.005, (z["names"][i], fit)
+        na = d["n_atoms"]
+        xs = [o.coords(lid, c, na) for c in confs]
+        ib = o.intramolecular_coords(lid, xs[0])
+        for c, x, (e_ref, lb_ref, ub_ref) in zip(confs, xs, remarks):
+            assert abs(o.eval_adjusted(lid, c, ib) - e_ref) <= 0.08, (z["names"][i], e_ref)
+            lb, ub = o.rmsd(lid, x.ravel(), xs[0].ravel())
+            assert abs(lb - lb_ref) <= 0.0015 and abs(ub - ub_ref) <= 0.0015, (z["names"][i], lb, ub)
+            n += 1
+    assert n == 342

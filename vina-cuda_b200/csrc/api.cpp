@@ -120,6 +120,7 @@ vd_status vd_destroy(vd_ctx* h) {
     cudaFree(c.d_fast);
     cudaFree(c.d_smooth);
     cudaFree(c.d_maps);
+    cudaFree(c.d_cells);
     cudaFree(c.d_rec);
     cudaFree(c.d_recd);
     cudaFree(c.d_cell_start);

@@ -166,8 +166,8 @@ int main(int argc, char** argv) {
     if (thread < 1000) die("thread must be at least 1000");
     const int search_depth = int(num("search_depth", 0));
     if (opt.count("search_depth") && search_depth < 1) die("search_depth must be 1 or greater");
-    if (int(num("rilc_bfgs", 1)) != 1)
-        std::fprintf(stderr, "WARNING: only the RILC-BFGS local search is implemented; using it\n");
+    const int rilc_bfgs = int(num("rilc_bfgs", 1));  // main.cpp:663: 1 = RILC-BFGS, 0 = dense BFGS
+    if (rilc_bfgs != 0 && rilc_bfgs != 1) die("rilc_bfgs must be 0 or 1");
     const double w_rot = num("weight_rot", 0.05846);
     const double weights[6] = {num("weight_gauss1", -0.035579), num("weight_gauss2", -0.005156),
                                num("weight_repulsion", 0.840245), num("weight_hydrophobic", -0.035069),
@@ -249,6 +249,7 @@ int main(int argc, char** argv) {
     sp.amplitude = 2.0;
     sp.min_rmsd = 1.0;
     sp.refine = 1;
+    sp.dense_bfgs = rilc_bfgs == 0;
     FILE* log = opt.count("log") ? std::fopen(opt["log"].c_str(), "w") : nullptr;
 
     struct Item {

@@ -126,6 +126,11 @@ struct Ctx {
     // grids
     float* d_maps = nullptr;              // [n_maps][nz][ny][pitch]
     size_t map_stride = 0;                // floats per map
+    // the same maps as trilinear cells for the evaluation kernels: per map
+    // [nz-1][ny-1][nx-1] cells of the 8 corner values (32 bytes, one sector),
+    // null when the box is too large for them (the kernels then read d_maps)
+    float* d_cells = nullptr;
+    size_t cell_stride = 0;               // floats per map
     int map_slot[kTypes];                 // xs type -> map index or -1
     int n_maps = 0;
     // direct-sum receptor cell list (non_cache): ~3 A cells over the box,

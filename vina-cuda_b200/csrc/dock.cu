@@ -2,7 +2,12 @@
 //
 // One warp runs one chain: `search_depth` steps of mutate -> RILC-BFGS ->
 // Metropolis (T = 1.2), re-optimising an accepted pose that beats the
-// chain's best, exactly the control flow of kernel2.cu:290-421.  Random
+// chain's best, exactly the control flow of kernel2.cu:290-421; or, with
+// vd_search_params.dense_bfgs (--rilc_bfgs 0), mutate -> dense BFGS ->
+// Metropolis as kernel2.cu:427-563, whose re-optimisation of an accepted
+// pose that beats the best is discarded there (it re-optimises a copy and
+// keeps the accepted pose and energy, kernel2.cu:526-552), so it is not run
+// here: same best poses and energies, fewer evaluations.  Random
 // numbers come from a Philox stream keyed by (seed, ligand, chain), so the
 // plain (one ligand per launch, one warp per chain) and the batched
 // (persistent, work queue over (ligand, chain) items) forms compute the same
@@ -61,13 +66,15 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
 // the large ones drop the register spills (ptxas: 84 bytes of spill stores
 // at 64, none at 128), which pays when a launch has few chains per SM.
 // Per-warp shared memory: the evaluation's arrays, then the poses xp, xo,
-// xt, xb (pad4(7 + ntors) floats each), then kChainWords chain scalars.
+// xt, xb (pad4(7 + ntors) floats each), then kChainWords chain scalars,
+// then (dense BFGS) the inverse Hessian and four pose-space vectors
+// (dense_floats).
 // chain scalar slots (ints, then floats)
 enum : int { kCsItem, kCsLig, kCsChain, kCsUid, kCsDepth, kCsSteps, kCsEvals0, kCsStep, kCsFloats };
 enum : int { kCfCurrent, kCfBest };
 static_assert(kCsFloats + kCfBest + 1 <= kChainWords, "chain scalars exceed their shared words");
 
-template <bool persistent, int MINB>
+template <bool persistent, int MINB, bool dense = false>
 __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -119,7 +126,20 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
             // pass 0 optimises the candidate; pass 1 re-optimises an accepted
             // candidate that beats the chain's best (one optimiser call site)
             for (int pass = 0; pass < 2; ++pass) {
-                const float ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, cs[kCsSteps], lane, evals);
+                float ce;
+                if (dense) {
+                    const int n = 6 + L.nt;
+                    float* H = reinterpret_cast<float*>(cs + kChainWords);  // after the chain scalars
+                    float* gc = H + pad4(n * n);
+                    float* pv = gc + pad4(n);
+                    float* yv = pv + pad4(n);
+                    float* mhy = yv + pad4(n);
+                    const GridInter gi{&p.G, p.ep.v_inter, p.ep.slope};
+                    ce = dense_bfgs<true>(L, s, H, gc, pv, yv, mhy, gi, p.smooth, p.ep.v_intra, p.ep.fix,
+                                          p.ep.inv_fix, cs[kCsSteps], lane, evals);
+                } else {
+                    ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, cs[kCsSteps], lane, evals);
+                }
                 const int stp = cs[kCsStep];
                 float tmp_e = cf[kCfCurrent], best_e = cf[kCfBest];
                 if (pass == 0) {
@@ -131,7 +151,11 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
                     tmp_e = ce;
                     __syncwarp();
                     if (lane == 0) cf[kCfCurrent] = tmp_e;
-                    if (!(tmp_e < best_e)) {
+                    if (dense || !(tmp_e < best_e)) {
+                        if (dense && tmp_e < best_e) {  // kernel2.cu:518-552: the accepted pose is the best
+                            if (lane == 0) cf[kCfBest] = tmp_e;
+                            copy_conf(s.m.x, xb, nc, lane);
+                        }
                         copy_conf(s.m.x, xt, nc, lane);
                         break;
                     }
@@ -173,6 +197,23 @@ DockFn dock_fn(int shape) {
         default: return dock_kernel<persistent, 8>;
     }
 }
+// Dense-BFGS search: built at the three register budgets the autotuner
+// explores (64 / 80 / 128); a pinned 48- or 40-register shape runs at 64.
+template <bool persistent>
+DockFn dense_dock_fn(int& shape) {
+    switch (shape) {
+        case 3: return dock_kernel<persistent, 6, true>;
+        case 4: return dock_kernel<persistent, 4, true>;
+        default: shape = 0; return dock_kernel<persistent, 8, true>;
+    }
+}
+
+// Shared-memory floats of the dense optimiser's state: H (n x n) and the
+// four vectors gc, pv, yv, mhy, n = 6 + ntors.
+int dense_floats(int ntors) {
+    const int n = 6 + ntors;
+    return pad4(n * n) + 4 * pad4(n);
+}
 
 }  // namespace
 
@@ -194,17 +235,20 @@ void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals) {
         if (kTunedShapes[i] == b.shape) c.dock_tune.report(b.tune_key, i, ms / double(evals));
 }
 
-// Heuristics of main.cpp:354-391 for RILC-BFGS (atoms = all ligand atoms).
+// Heuristics of main.cpp:354-391 (atoms = all ligand atoms): search depth
+// (0.24 atoms + 0.29 torsions - 3.41) x 2 and (30 + atoms)/3 BFGS steps for
+// RILC-BFGS; x 2.4 and (25 + atoms)/3 for dense BFGS (--rilc_bfgs 0).
 void search_defaults(const HostLigand& L, const vd_search_params& sp, int& depth, int& bfgs_steps) {
+    const bool dense = sp.dense_bfgs != 0;
     depth = sp.search_depth;
     if (depth < 0) {  // no MC steps: each chain returns its initial pose
         depth = 0;
     } else if (depth == 0) {
-        double t = (0.24 * L.n_all_atoms + 0.29 * L.h.ntors - 3.41) * 2;
+        double t = (0.24 * L.n_all_atoms + 0.29 * L.h.ntors - 3.41) * (dense ? 2.4 : 2.0);
         if (t < 1) t = 1;
         depth = int(t);
     }
-    bfgs_steps = sp.max_bfgs_steps > 0 ? sp.max_bfgs_steps : int(unsigned(30 + L.n_all_atoms) / 3);
+    bfgs_steps = sp.max_bfgs_steps > 0 ? sp.max_bfgs_steps : int(unsigned((dense ? 25 : 30) + L.n_all_atoms) / 3);
 }
 
 // Host side of a docking launch: checks, heuristics, device scratch layout
@@ -236,7 +280,8 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
         uid[i] = uint32_t(ligs[i]);
         search_defaults(L, sp, depth[i], steps[i]);
         prefix[i + 1] = prefix[i] + sp.n_chains;
-        max_wf = std::max(max_wf, lig_warp_floats(L) + 4 * pad4(7 + L.h.ntors) + kChainWords);
+        max_wf = std::max(max_wf, lig_warp_floats(L) + 4 * pad4(7 + L.h.ntors) + kChainWords +
+                                      (sp.dense_bfgs ? dense_floats(L.h.ntors) : 0));
         max_nt = std::max(max_nt, L.h.ntors);
     }
     const int items = prefix[n];
@@ -302,11 +347,13 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     p.warps_per_block = wpb;
     out.tune_key = (uint64_t(persistent) << 40) | (uint64_t(ceil_log2(uint64_t(items))) << 32) |
                    uint64_t(max_wf > 1024);  // above 4 KB per chain, shared memory caps the occupancy
+    out.tune_key |= uint64_t(sp.dense_bfgs != 0) << 41;
     out.tuned = sp.launch_shape == 0;
     out.shape = dock_shape_for(c, sp, out.tune_key);
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
-    const DockFn k = persistent ? dock_fn<true>(out.shape) : dock_fn<false>(out.shape);
+    const DockFn k = sp.dense_bfgs ? (persistent ? dense_dock_fn<true>(out.shape) : dense_dock_fn<false>(out.shape))
+                                   : (persistent ? dock_fn<true>(out.shape) : dock_fn<false>(out.shape));
     VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     int blocks = (items + wpb - 1) / wpb;
     if (persistent) {
@@ -498,12 +545,12 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     p.queue = nullptr;  // one warp per chain: no work queue
     p.evals = d_cnt;
     p.lig_evals = d_cnt + 1;
-    p.warp_floats = lig_warp_floats(L) + 4 * pad4(nc) + kChainWords;
+    p.warp_floats = lig_warp_floats(L) + 4 * pad4(nc) + kChainWords + (sp->dense_bfgs ? dense_floats(L.h.ntors) : 0);
     const int wpb = 4;
     const size_t smem = size_t(p.warp_floats) * wpb * sizeof(float);
     VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "vd_mc_chains_noalloc: ligand too large for the kernel");
     p.warps_per_block = wpb;
-    auto k = dock_kernel<false, 8>;
+    auto k = sp->dense_bfgs ? dock_kernel<false, 8, true> : dock_kernel<false, 8>;
     VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     k<<<(n + wpb - 1) / wpb, 32 * wpb, smem, c.stream>>>(p);
     VD_CUDA(cudaGetLastError());

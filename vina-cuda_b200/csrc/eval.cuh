@@ -36,6 +36,7 @@ namespace vd {
 
 struct MapView {
     const float* map[kTypes];   // per XS type (nullptr if not built)
+    const float* cell[kTypes];  // same maps as 32-byte corner cells (nullptr: read map)
     float init[3], factor[3], finv[3], dmo[3];
     int32_t n[3];
     int32_t pitch;
@@ -213,8 +214,37 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
 // penalty.  Outside the box a coordinate is clamped to the nearest cell
 // (fraction 0 below, 1 above), the gradient component is replaced by
 // slope * region and the penalty adds slope * distance outside.
-__device__ __forceinline__ float grid_term(const MapView& G, const float* map, float px, float py, float pz,
-                                           float v, float slope, float& gx, float& gy, float& gz) {
+// The eight corners of trilinear cell (a0, a1, a2): from the corner-cell
+// layout, one 256-bit load of one 32-byte sector (x fastest, then y, then z:
+// f000 f100 f010 f110 f001 f101 f011 f111); else eight loads from the map.
+struct Corners {
+    float f000, f100, f010, f110, f001, f101, f011, f111;
+};
+__device__ __forceinline__ Corners load_corners(const MapView& G, const float* map, const float* cell, int a0, int a1,
+                                                int a2) {
+    Corners k;
+    if (cell) {
+        const float* c = cell + ((size_t(a2) * (G.n[1] - 1) + a1) * (G.n[0] - 1) + a0) * 8;
+        unsigned long long w0, w1, w2, w3;
+        asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];" : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3) : "l"(c));
+        k.f000 = __int_as_float(int(w0 & 0xffffffffull)); k.f100 = __int_as_float(int(w0 >> 32));
+        k.f010 = __int_as_float(int(w1 & 0xffffffffull)); k.f110 = __int_as_float(int(w1 >> 32));
+        k.f001 = __int_as_float(int(w2 & 0xffffffffull)); k.f101 = __int_as_float(int(w2 >> 32));
+        k.f011 = __int_as_float(int(w3 & 0xffffffffull)); k.f111 = __int_as_float(int(w3 >> 32));
+    } else {
+        const size_t row = size_t(G.pitch);
+        const size_t plane = row * size_t(G.n[1]);
+        const float* b = map + size_t(a2) * plane + size_t(a1) * row + a0;
+        k.f000 = __ldg(b); k.f100 = __ldg(b + 1);
+        k.f010 = __ldg(b + row); k.f110 = __ldg(b + row + 1);
+        k.f001 = __ldg(b + plane); k.f101 = __ldg(b + plane + 1);
+        k.f011 = __ldg(b + plane + row); k.f111 = __ldg(b + plane + row + 1);
+    }
+    return k;
+}
+
+__device__ __forceinline__ float grid_term(const MapView& G, const float* map, const float* cell, float px, float py,
+                                           float pz, float v, float slope, float& gx, float& gy, float& gz) {
     const float pc[3] = {px, py, pz};
     float fr[3], miss = 0.f, reg[3];
     int a[3];
@@ -230,13 +260,9 @@ __device__ __forceinline__ float grid_term(const MapView& G, const float* map, f
         fr[d] = (s >= G.dmo[d]) ? 1.f : sc - float(ai);
     }
     const float penalty = slope * miss;
-    const size_t row = size_t(G.pitch);
-    const size_t plane = row * size_t(G.n[1]);
-    const float* b = map + size_t(a[2]) * plane + size_t(a[1]) * row + a[0];
-    const float f000 = __ldg(b), f100 = __ldg(b + 1);
-    const float f010 = __ldg(b + row), f110 = __ldg(b + row + 1);
-    const float f001 = __ldg(b + plane), f101 = __ldg(b + plane + 1);
-    const float f011 = __ldg(b + plane + row), f111 = __ldg(b + plane + row + 1);
+    const Corners k = load_corners(G, map, cell, a[0], a[1], a[2]);
+    const float f000 = k.f000, f100 = k.f100, f010 = k.f010, f110 = k.f110;
+    const float f001 = k.f001, f101 = k.f101, f011 = k.f011, f111 = k.f111;
     const float x = fr[0], y = fr[1], z = fr[2];
     const float mx = 1.f - x, my = 1.f - y, mz = 1.f - z;
     float f = f000 * mx * my * mz + f100 * x * my * mz + f010 * mx * y * mz + f110 * x * y * mz +
@@ -268,7 +294,7 @@ struct GridInter {
             return 0.f;
         }
 #endif
-        return grid_term(*G, G->map[t], px, py, pz, v, slope, gx, gy, gz);
+        return grid_term(*G, G->map[t], G->cell[t], px, py, pz, v, slope, gx, gy, gz);
     }
 };
 

@@ -259,6 +259,36 @@ __global__ void __launch_bounds__(32 * TZ, 16 / TZ) grid_build_kernel(GridParams
     }
 }
 
+// Corner cells for the evaluation kernels: cell (x, y, z) of map j holds the
+// map values at its 8 corners (x fastest, then y, then z), 32 bytes, so a
+// trilinear lookup reads one sector instead of eight scattered floats.  One
+// thread per cell; consecutive threads write consecutive cells.
+__global__ void __launch_bounds__(256) corner_cells_kernel(const float* maps, size_t map_stride, float* cells,
+                                                           size_t cell_stride, int n_maps, int nx, int ny, int nz,
+                                                           int pitch) {
+    const int cx = nx - 1, cy = ny - 1, cz = nz - 1;
+    const size_t per_map = size_t(cx) * cy * cz;
+    const size_t total = per_map * size_t(n_maps);
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
+        const int j = int(i / per_map);
+        const size_t r = i - size_t(j) * per_map;
+        const int x = int(r % size_t(cx));
+        const size_t yz = r / size_t(cx);
+        const int y = int(yz % size_t(cy)), z = int(yz / size_t(cy));
+        const float* b = maps + size_t(j) * map_stride + (size_t(z) * ny + y) * pitch + x;
+        const size_t row = size_t(pitch), plane = row * size_t(ny);
+        const float4 lo = make_float4(b[0], b[1], b[row], b[row + 1]);
+        const float4 hi = make_float4(b[plane], b[plane + 1], b[plane + row], b[plane + row + 1]);
+        float4* d = reinterpret_cast<float4*>(cells + size_t(j) * cell_stride + r * 8);
+        d[0] = lo;
+        d[1] = hi;
+    }
+}
+
+// Corner cells are built when all of them fit in this many bytes (a 150 A
+// box of 17 maps is about 11 GB); larger boxes keep the plain maps only.
+constexpr size_t kMaxCellBytes = size_t(16) << 30;
+
 }  // namespace
 }  // namespace vd
 
@@ -360,6 +390,7 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
     const size_t bytes_start = start.size() * sizeof(int32_t);
     const size_t bytes_lut = lut.size() * sizeof(float);
     dev_release(c, c.d_maps);
+    dev_release(c, c.d_cells);
     c.n_maps = 0;
     for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;
     vd_status st0 = dev_alloc(c, &c.d_maps, bytes_maps, "vd_build_grids: maps");
@@ -430,6 +461,28 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
         c.stats.grid_shape = shape + 1;
     }
     c.stats.grid_ms = best_ms;
+    // corner cells of the new maps (timed separately: cells_ms)
+    const size_t n_cells_map = size_t(g.n[0] - 1) * (g.n[1] - 1) * (g.n[2] - 1);
+    const size_t bytes_cells = n_cells_map * 8 * sizeof(float) * nt;
+    c.stats.cells_ms = 0;
+    if (bytes_cells <= kMaxCellBytes) {
+        st = dev_alloc(c, &c.d_cells, bytes_cells, "vd_build_grids: corner cells");
+        if (st != VD_OK) return st;
+        c.cell_stride = n_cells_map * 8;
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device);
+        const size_t total = n_cells_map * nt;
+        const int blocks = int(std::min<size_t>((total + 255) / 256, size_t(sms) * 8));
+        VD_CUDA(cudaEventRecord(c.ev0, c.stream));
+        corner_cells_kernel<<<blocks, 256, 0, c.stream>>>(c.d_maps, map_stride, c.d_cells, c.cell_stride, nt, g.n[0],
+                                                            g.n[1], g.n[2], g.pitch);
+        VD_CUDA(cudaGetLastError());
+        VD_CUDA(cudaEventRecord(c.ev1, c.stream));
+        VD_CUDA(cudaEventSynchronize(c.ev1));
+        float ms = 0;
+        VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
+        c.stats.cells_ms = ms;
+    }
     c.map_stride = map_stride;
     c.n_maps = nt;
     for (int i = 0; i < kTypes; ++i) c.map_slot[i] = -1;

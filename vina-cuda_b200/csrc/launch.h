@@ -8,8 +8,10 @@ namespace vd {
 
 inline vd_status make_map_view(Ctx& c, MapView& G) {
     VD_CHECK(c.n_maps > 0, VD_ERR_ARG, "grid maps not built (vd_build_grids)");
-    for (int t = 0; t < kTypes; ++t)
+    for (int t = 0; t < kTypes; ++t) {
         G.map[t] = (c.map_slot[t] >= 0) ? c.d_maps + size_t(c.map_slot[t]) * c.map_stride : nullptr;
+        G.cell[t] = (c.map_slot[t] >= 0 && c.d_cells) ? c.d_cells + size_t(c.map_slot[t]) * c.cell_stride : nullptr;
+    }
     for (int d = 0; d < 3; ++d) {
         G.init[d] = float(c.geom.init[d]);
         G.factor[d] = float(c.geom.factor[d]);

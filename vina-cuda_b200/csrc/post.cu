@@ -197,74 +197,6 @@ struct RefineParams {
     int32_t skip_invalid;       // leave poses whose e_out is FLT_MAX untouched
 };
 
-// bfgs.h:95-140 (dense BFGS, Armijo backtracking), warp-parallel; H in smem.
-template <class Inter>
-__device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, float* gc, float* pv, float* yv,
-                           float* mhy, const Inter& inter, const float4* smooth, float v_intra, float fix,
-                           float inv_fix, int max_steps, int lane, int& evals) {
-    const int n = 6 + L.nt, nc = 7 + L.nt;
-    for (int i = lane; i < n * n; i += 32) H[i] = (i / n == i % n) ? 1.f : 0.f;
-    float f0 = eval_pose_t<true>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
-    ++evals;
-    for (int i = lane; i < n; i += 32) gc[i] = s.m.g[i];
-    const float f_orig = f0;
-    copy_conf(s.m.x, s.xo, nc, lane);
-    for (int step = 0; step < max_steps; ++step) {
-        for (int i = lane; i < n; i += 32) {  // p = -H g
-            float sum = 0.f;
-            for (int j = 0; j < n; ++j) sum += H[i * n + j] * gc[j];
-            pv[i] = -sum;
-        }
-        __syncwarp();
-        copy_conf(s.m.x, s.xp, nc, lane);
-        const Vec2 p = vload(pv, n, lane), g = vload(gc, n, lane);
-        const float pg = vdot(p, g);
-        float alpha = 1.f, f1 = 0.f;
-        for (int trial = 0; trial < 10; ++trial) {  // line_search, bfgs.h:65-82
-            conf_step(s.xp, s.m.x, p, alpha, L.nt, lane);
-            f1 = eval_pose_t<true>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
-            ++evals;
-            if (f1 - f0 < 0.0001f * alpha * pg) break;
-            alpha *= 0.5f;
-        }
-        const Vec2 gn = vload(s.m.g, n, lane);
-        const Vec2 y = {gn.a - g.a, gn.b - g.b};
-        f0 = f1;
-        if (!(sqrtf(vdot(g, g)) >= 1e-5f)) break;
-        for (int i = lane; i < n; i += 32) { gc[i] = s.m.g[i]; yv[i] = s.m.g[i] - (i < 32 ? g.a : g.b); }
-        __syncwarp();
-        if (step == 0) {
-            const float yy = vdot(y, y);
-            if (fabsf(yy) > FLT_EPSILON) {
-                const float dg = alpha * vdot(y, p) / yy;
-                for (int i = lane; i < n; i += 32) H[i * n + i] = dg;
-                __syncwarp();
-            }
-        }
-        const float yp = vdot(y, p);  // bfgs_update, bfgs.h:49-63
-        if (alpha * yp < FLT_EPSILON) continue;
-        for (int i = lane; i < n; i += 32) {
-            float sum = 0.f;
-            for (int j = 0; j < n; ++j) sum += H[i * n + j] * yv[j];
-            mhy[i] = -sum;
-        }
-        __syncwarp();
-        const float yhy = -vdot(y, vload(mhy, n, lane));
-        const float r = 1.f / (alpha * yp);
-        const float c2 = alpha * alpha * (r * r * yhy + r);
-        for (int idx = lane; idx < n * n; idx += 32) {
-            const int i = idx / n, j = idx % n;
-            H[idx] += alpha * r * (mhy[i] * pv[j] + mhy[j] * pv[i]) + c2 * pv[i] * pv[j];
-        }
-        __syncwarp();
-    }
-    if (!(f0 <= f_orig)) {
-        f0 = f_orig;
-        copy_conf(s.xo, s.m.x, nc, lane);
-    }
-    return f0;
-}
-
 constexpr int kRefineWarps = 4;
 
 __device__ __forceinline__ bool m_out(float v, double b, double e) {
@@ -468,6 +400,61 @@ __global__ void gather_kernel(const int32_t* kept, const float* conf, const floa
     if (threadIdx.x == 0) re[slot] = item >= 0 ? e[item] : FLT_MAX;
 }
 
+// model.cpp:1485-1523: RMSD upper bound (each heavy atom to the same atom)
+// and lower bound (each heavy atom to the nearest atom of the same element,
+// the larger of the two directions) between heavy-atom coordinate sets a and
+// b ([na][3] floats); sums in double.  Same value in every lane.
+__device__ void rmsd_bounds(const LigView& L, const float* a, const float* b, int lane, double& lb, double& ub) {
+    double su = 0, s1 = 0, s2 = 0;
+    for (int i = lane; i < L.na; i += 32) {
+        const int ei = (__float_as_int(L.atoms[i].w) >> 16) & 0xff;
+        double d2 = 0, m1 = DBL_MAX, m2 = DBL_MAX;
+        for (int d = 0; d < 3; ++d) d2 += double(a[3 * i + d] - b[3 * i + d]) * double(a[3 * i + d] - b[3 * i + d]);
+        for (int q = 0; q < L.na; ++q) {
+            if (((__float_as_int(L.atoms[q].w) >> 16) & 0xff) != ei) continue;
+            double t1 = 0, t2 = 0;
+            for (int d = 0; d < 3; ++d) {
+                t1 += double(a[3 * i + d] - b[3 * q + d]) * double(a[3 * i + d] - b[3 * q + d]);
+                t2 += double(b[3 * i + d] - a[3 * q + d]) * double(b[3 * i + d] - a[3 * q + d]);
+            }
+            m1 = fmin(m1, t1);
+            m2 = fmin(m2, t2);
+        }
+        su += d2; s1 += m1; s2 += m2;
+    }
+    su = warp_sum_d(su); s1 = warp_sum_d(s1); s2 = warp_sum_d(s2);
+    ub = sqrt(su / L.na);
+    lb = fmax(sqrt(s1 / L.na), sqrt(s2 / L.na));
+}
+
+// RMSD bounds of poses to pose 0 (vd_rmsd_bounds): heavy-atom coordinates in
+// double, stored as floats as the output stage stores its kept modes.
+__global__ void __launch_bounds__(32) rmsd_poses_kernel(const float4* pool, const int64_t* off, const float* poses,
+                                                         int n, int stride, double* out) {
+    extern __shared__ double smemd[];
+    const int lane = threadIdx.x;
+    const LigView L = lig_view(pool, off[0]);
+    double* nd = smemd;
+    double* c = nd + 16 * L.nn;
+    float* k0 = reinterpret_cast<float*>(c + 3 * L.na);
+    float* ki = k0 + 3 * L.na;
+    coords_d(L, poses, nd, c, lane);
+    for (int a = lane; a < 3 * L.na; a += 32) k0[a] = float(c[a]);
+    __syncwarp();
+    for (int i = 0; i < n; ++i) {
+        coords_d(L, poses + size_t(i) * stride, nd, c, lane);
+        for (int a = lane; a < 3 * L.na; a += 32) ki[a] = float(c[a]);
+        __syncwarp();
+        double lb, ub;
+        rmsd_bounds(L, ki, k0, lane, lb, ub);
+        if (lane == 0) {
+            out[2 * i] = lb;
+            out[2 * i + 1] = ub;
+        }
+        __syncwarp();
+    }
+}
+
 // Adjusted score and intramolecular energy of up to 20 poses (vd_score).
 __global__ void __launch_bounds__(32) score_poses_kernel(const float4* pool, const int64_t* off, const float* poses,
                                                           int n, int stride, RecView R, const double* fastd,
@@ -563,31 +550,13 @@ __global__ void __launch_bounds__(32) score_kernel(ScoreParams p) {
     __syncwarp();
     // outputs with RMSD bounds to mode 1 (model.cpp:1485-1523)
     for (int j = 0; j < nk; ++j) {
-        const float* a = kc + size_t(j) * 3 * L.na;
-        const float* b = kc;
-        double ub = 0, lb1 = 0, lb2 = 0;
-        for (int i = lane; i < L.na; i += 32) {
-            const int ei = (__float_as_int(L.atoms[i].w) >> 16) & 0xff;
-            double d2 = 0, m1 = DBL_MAX, m2 = DBL_MAX;
-            for (int d = 0; d < 3; ++d) d2 += double(a[3 * i + d] - b[3 * i + d]) * double(a[3 * i + d] - b[3 * i + d]);
-            for (int q = 0; q < L.na; ++q) {
-                if (((__float_as_int(L.atoms[q].w) >> 16) & 0xff) != ei) continue;
-                double t1 = 0, t2 = 0;
-                for (int d = 0; d < 3; ++d) {
-                    t1 += double(a[3 * i + d] - b[3 * q + d]) * double(a[3 * i + d] - b[3 * q + d]);
-                    t2 += double(b[3 * i + d] - a[3 * q + d]) * double(b[3 * i + d] - a[3 * q + d]);
-                }
-                m1 = fmin(m1, t1);
-                m2 = fmin(m2, t2);
-            }
-            ub += d2; lb1 += m1; lb2 += m2;
-        }
-        ub = warp_sum_d(ub); lb1 = warp_sum_d(lb1); lb2 = warp_sum_d(lb2);
+        double lb, ub;
+        rmsd_bounds(L, kc + size_t(j) * 3 * L.na, kc, lane, lb, ub);
         const int i = kept[j];
         if (lane == 0) {
             out->energy[j] = float(adj[i]);
-            out->rmsd_ub[j] = float(sqrt(ub / L.na));
-            out->rmsd_lb[j] = float(fmax(sqrt(lb1 / L.na), sqrt(lb2 / L.na)));
+            out->rmsd_ub[j] = float(ub);
+            out->rmsd_lb[j] = float(lb);
         }
         for (int q = lane; q < 7 + L.nt; q += 32) out->pose[j][q] = poses[size_t(i) * p.stride + q];
     }
@@ -998,7 +967,8 @@ vd_status vd_dock_batched(vd_ctx* h, const int32_t* ligs, int32_t n, const vd_se
         int depth = 0, steps = 0;
         search_defaults(L, *sp, depth, steps);
         order[i] = i;
-        cost[i] = double(std::max(depth, 1)) * steps * (32.0 * L.h.n_atoms + 16.0 * L.h.n_pairs);
+        // depth 0 here means no MC step (a negative search_depth): one evaluation's bytes
+        cost[i] = double(depth > 0 ? double(depth) * steps : 1.0) * (32.0 * L.h.n_atoms + 16.0 * L.h.n_pairs);
     }
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
     std::vector<int> v(n);
@@ -1093,6 +1063,39 @@ vd_status vd_score(vd_ctx* h, int32_t lig, int32_t n, const float* poses, float*
     for (int i = 0; i < n; ++i) {
         if (adjusted) adjusted[i] = float(o[2 * i]);
         if (intra) intra[i] = float(o[2 * i + 1]);
+    }
+    return VD_OK;
+}
+
+vd_status vd_rmsd_bounds(vd_ctx* h, int32_t lig, int32_t n, const float* poses, float* lb_out, float* ub_out) {
+    VD_CHECK(h && poses && lb_out && ub_out && n >= 0, VD_ERR_ARG, "vd_rmsd_bounds: bad arguments");
+    Ctx& c = h->c;
+    VD_CHECK(lig >= 0 && lig < int(c.ligs.size()), VD_ERR_ARG, "vd_rmsd_bounds: bad ligand id");
+    if (n == 0) return VD_OK;
+    VD_CUDA(cudaSetDevice(c.device));
+    vd_status st = sync_pool(&c);
+    if (st != VD_OK) return st;
+    const HostLigand& L = c.ligs[lig];
+    const int nc = 7 + L.h.ntors;
+    st = ensure_scratch(&c, al256(size_t(n) * nc * 4) + al256(size_t(n) * 16) + 512);
+    if (st != VD_OK) return st;
+    char* s = static_cast<char*>(c.d_scratch);
+    float* d_p = reinterpret_cast<float*>(s); s += al256(size_t(n) * nc * 4);
+    double* d_o = reinterpret_cast<double*>(s); s += al256(size_t(n) * 16);
+    int64_t* d_off = reinterpret_cast<int64_t*>(s);
+    VD_CUDA(cudaMemcpyAsync(d_p, poses, size_t(n) * nc * 4, cudaMemcpyHostToDevice, c.stream));
+    const int64_t off = L.pool_offset;
+    VD_CUDA(cudaMemcpyAsync(d_off, &off, 8, cudaMemcpyHostToDevice, c.stream));
+    const size_t smem = size_t(16 * L.h.n_nodes + 3 * L.h.n_atoms) * 8 + size_t(6 * L.h.n_atoms) * 4;
+    rmsd_poses_kernel<<<1, 32, smem, c.stream>>>(c.d_pool, d_off, d_p, n, nc, d_o);
+    VD_CUDA(cudaGetLastError());
+    std::vector<double> o(size_t(n) * 2);
+    VD_CUDA(cudaMemcpyAsync(o.data(), d_o, o.size() * 8, cudaMemcpyDeviceToHost, c.stream));
+    VD_CUDA(cudaStreamSynchronize(c.stream));
+    { const vd_status cs = take_device_checks("RMSD kernel"); if (cs != VD_OK) return cs; }
+    for (int i = 0; i < n; ++i) {
+        lb_out[i] = float(o[2 * i]);
+        ub_out[i] = float(o[2 * i + 1]);
     }
     return VD_OK;
 }

@@ -198,6 +198,80 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
     return fx;
 }
 
+// bfgs.h:95-140 (dense BFGS, Armijo backtracking line_search 65-82,
+// bfgs_update 49-63) and its GPU form bfgs_optimized
+// (quasi_newton.cuh:2391-2499, line_search_optimized 1859-1916), warp-
+// parallel: the inverse Hessian H (n x n, full storage) and the vectors gc,
+// pv, yv, mhy (n floats each) in the warp's shared memory.  Used by the
+// refinement (direct-sum score) and by the Monte-Carlo search with
+// --rilc_bfgs 0 (grid maps).  pair_atomics as in eval_pose_t.
+template <bool pair_atomics = false, class Inter>
+__device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, float* gc, float* pv, float* yv,
+                           float* mhy, const Inter& inter, const float4* smooth, float v_intra, float fix,
+                           float inv_fix, int max_steps, int lane, int& evals) {
+    const int n = 6 + L.nt, nc = 7 + L.nt;
+    for (int i = lane; i < n * n; i += 32) H[i] = (i / n == i % n) ? 1.f : 0.f;
+    float f0 = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
+    ++evals;
+    for (int i = lane; i < n; i += 32) gc[i] = s.m.g[i];
+    const float f_orig = f0;
+    copy_conf(s.m.x, s.xo, nc, lane);
+    for (int step = 0; step < max_steps; ++step) {
+        for (int i = lane; i < n; i += 32) {  // p = -H g
+            float sum = 0.f;
+            for (int j = 0; j < n; ++j) sum += H[i * n + j] * gc[j];
+            pv[i] = -sum;
+        }
+        __syncwarp();
+        copy_conf(s.m.x, s.xp, nc, lane);
+        const Vec2 p = vload(pv, n, lane), g = vload(gc, n, lane);
+        const float pg = vdot(p, g);
+        float alpha = 1.f, f1 = 0.f;
+        for (int trial = 0; trial < 10; ++trial) {  // line_search, bfgs.h:65-82
+            conf_step(s.xp, s.m.x, p, alpha, L.nt, lane);
+            f1 = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
+            ++evals;
+            if (f1 - f0 < 0.0001f * alpha * pg) break;
+            alpha *= 0.5f;
+        }
+        const Vec2 gn = vload(s.m.g, n, lane);
+        const Vec2 y = {gn.a - g.a, gn.b - g.b};
+        f0 = f1;
+        if (!(sqrtf(vdot(g, g)) >= 1e-5f)) break;
+        for (int i = lane; i < n; i += 32) { gc[i] = s.m.g[i]; yv[i] = s.m.g[i] - (i < 32 ? g.a : g.b); }
+        __syncwarp();
+        if (step == 0) {
+            const float yy = vdot(y, y);
+            if (fabsf(yy) > FLT_EPSILON) {
+                const float dg = alpha * vdot(y, p) / yy;
+                for (int i = lane; i < n; i += 32) H[i * n + i] = dg;
+                __syncwarp();
+            }
+        }
+        const float yp = vdot(y, p);  // bfgs_update, bfgs.h:49-63
+        if (alpha * yp < FLT_EPSILON) continue;
+        for (int i = lane; i < n; i += 32) {
+            float sum = 0.f;
+            for (int j = 0; j < n; ++j) sum += H[i * n + j] * yv[j];
+            mhy[i] = -sum;
+        }
+        __syncwarp();
+        const float yhy = -vdot(y, vload(mhy, n, lane));
+        const float r = 1.f / (alpha * yp);
+        const float c2 = alpha * alpha * (r * r * yhy + r);
+        for (int idx = lane; idx < n * n; idx += 32) {
+            const int i = idx / n, j = idx % n;
+            H[idx] += alpha * r * (mhy[i] * pv[j] + mhy[j] * pv[i]) + c2 * pv[i] * pv[j];
+        }
+        __syncwarp();
+    }
+    if (!(f0 <= f_orig)) {
+        f0 = f_orig;
+        copy_conf(s.xo, s.m.x, nc, lane);
+    }
+    return f0;
+}
+
 // Random initial pose (conf.h:137-140 rigid_conf::randomize, torsions in
 // [-pi, pi]) from the chain's Philox stream; written to x.
 __device__ __forceinline__ void init_pose(float* x, int nt, uint32_t seed, uint32_t lig, uint32_t chain,

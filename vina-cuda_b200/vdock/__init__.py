@@ -42,7 +42,8 @@ class SearchParams(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("n_chains", C.c_int32), ("search_depth", C.c_int32),
                 ("max_bfgs_steps", C.c_int32), ("num_modes", C.c_int32), ("energy_range", C.c_double),
                 ("hunt_cap", C.c_double * 3), ("temperature", C.c_double), ("amplitude", C.c_double),
-                ("min_rmsd", C.c_double), ("refine", C.c_int32), ("launch_shape", C.c_int32)]
+                ("min_rmsd", C.c_double), ("refine", C.c_int32), ("launch_shape", C.c_int32),
+                ("dense_bfgs", C.c_int32)]
 
 
 class DockResult(C.Structure):
@@ -56,7 +57,7 @@ class Stats(C.Structure):
                 ("post_ms", C.c_double), ("dock_warps_per_block", C.c_int32), ("dock_blocks", C.c_int32),
                 ("dock_shape", C.c_int32), ("grid_shape", C.c_int32), ("graph_launches", C.c_int64),
                 ("graph_instantiations", C.c_int64), ("scoring_ms", C.c_double), ("device_bytes", C.c_int64),
-                ("pair_force_scale", C.c_double)]
+                ("pair_force_scale", C.c_double), ("cells_ms", C.c_double)]
 
 
 EXPORTS = [
@@ -66,7 +67,7 @@ EXPORTS = [
     "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
     "vd_pose_coords",
     "vd_local_opt", "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score",
-    "vd_get_tables", "vd_pdbqt_ligand", "vd_pdbqt_receptor", "vd_pdbqt_write_model", "vd_pdbqt_free",
+    "vd_rmsd_bounds", "vd_get_tables", "vd_pdbqt_ligand", "vd_pdbqt_receptor", "vd_pdbqt_write_model", "vd_pdbqt_free",
     "vd_conf_to_coords",
 ]
 
@@ -106,13 +107,14 @@ def lib():
         L.vd_dock_batched.argtypes = [_vp, _ip, C.c_int32, C.POINTER(SearchParams), C.POINTER(DockResult)]
         L.vd_refine.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.c_int32, _fp]
         L.vd_score.argtypes = [_vp, C.c_int32, C.c_int32, _fp, _fp, _fp]
+        L.vd_rmsd_bounds.argtypes = [_vp, C.c_int32, C.c_int32, _fp, _fp, _fp]
         L.vd_get_tables.argtypes = [_vp, _dp, _dp, _dp]
         for name in ("vd_create", "vd_destroy", "vd_get_stats", "vd_set_memory_cap", "vd_set_scoring", "vd_set_scoring_device",
                      "vd_set_receptor",
                      "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand",
                      "vd_ligand_info", "vd_clear_ligands", "vd_energy", "vd_energy_grad",
                      "vd_energy_grad_device", "vd_energy_device", "vd_pose_coords", "vd_local_opt",
-                     "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_get_tables"):
+                     "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score", "vd_rmsd_bounds", "vd_get_tables"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -140,7 +142,7 @@ def _f(a):
 
 def search_params(seed=0, n_chains=8192, search_depth=0, max_bfgs_steps=0, num_modes=9,
                   energy_range=3.0, hunt_cap=(10, 10, 10), temperature=1.2, amplitude=2.0,
-                  min_rmsd=1.0, refine=1, launch_shape=0):
+                  min_rmsd=1.0, refine=1, launch_shape=0, dense_bfgs=0):
     s = SearchParams()
     s.seed, s.n_chains, s.search_depth, s.max_bfgs_steps = seed, n_chains, search_depth, max_bfgs_steps
     s.num_modes, s.energy_range = num_modes, energy_range
@@ -148,6 +150,7 @@ def search_params(seed=0, n_chains=8192, search_depth=0, max_bfgs_steps=0, num_m
         s.hunt_cap[i] = hunt_cap[i]
     s.temperature, s.amplitude, s.min_rmsd, s.refine = temperature, amplitude, min_rmsd, refine
     s.launch_shape = launch_shape
+    s.dense_bfgs = int(dense_bfgs)
     return s
 
 
@@ -353,3 +356,12 @@ class Context:
         i, ipp = _f(np.zeros(n, dtype=np.float32))
         _check(self.L.vd_score(self.h, lig, n, pp, ap, ipp))
         return a, i
+
+    def rmsd_bounds(self, lig, poses):
+        """RMSD lower and upper bounds of each pose to pose 0 (heavy atoms)."""
+        p, pp = _f(poses)
+        n = p.shape[0]
+        lb, lbp = _f(np.zeros(n, dtype=np.float32))
+        ub, ubp = _f(np.zeros(n, dtype=np.float32))
+        _check(self.L.vd_rmsd_bounds(self.h, lig, n, pp, lbp, ubp))
+        return lb, ub
