@@ -132,6 +132,27 @@ def lig_bytes(lig):
 # figure by the evaluations of each launch.
 DOCK_DRAM_BYTES_PER_EVAL = {1: 499.0, 4: 392.0, 5: 336.0}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
+# L1 data-pipe (LSU) wavefronts of one grid build of this workload (188^3
+# points x 8 maps, 8,000-atom receptor), from the ncu capture summarised in
+# profiles/grid_build_kernel_70A_8types.txt (l1tex__data_pipe_lsu_wavefronts.sum
+# of one grid_build_kernel launch).  The kernel's limit is that pipe: one
+# wavefront per SM per cycle; every in-range (point, receptor atom) pair reads
+# one 32-byte table row, one wavefront.
+GRID_L1_WAVEFRONTS = None
+
+
+def grid_l1_roof(ms, clk, device):
+    """Fraction of the L1 data-pipe wavefront roof the grid build reaches:
+    wavefronts per build (ncu) / (build time x SMs x SM clock x 1 wavefront
+    per SM per cycle), at the median SM clock sampled during the timed region."""
+    if GRID_L1_WAVEFRONTS is None:
+        return {"frac_of_l1_wavefront_roof": None}
+    import torch
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = sms * mhz * 1e6  # wavefronts per second
+    return {"l1_wavefronts": GRID_L1_WAVEFRONTS, "l1_wavefronts_per_s": GRID_L1_WAVEFRONTS / (ms / 1e3),
+            "frac_of_l1_wavefront_roof": GRID_L1_WAVEFRONTS / (ms / 1e3) / peak}
 
 
 def peaks():
@@ -142,12 +163,13 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(xyz, xs, ligs, chains_per_lig, n_sample, orc=None):
+def cpu_baseline(xyz, xs, ligs, chains_per_lig, n_sample, orc=None, warm=None):
     """Oracle port (double precision restatement of the reference's search,
     clustering and refinement) timed on the host cores on a bounded sample
     of the same workload: n_sample whole ligands (all chains, top-20
     refinement).  orc: an oracle with this receptor, box and maps already
-    set up (its grid build is then not timed again)."""
+    set up (its grid build is then not timed again); warm: a ligand docked
+    untimed first (thread start-up, first-touch page faults)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle_lib
     from vdock import synth
@@ -158,6 +180,10 @@ def cpu_baseline(xyz, xs, ligs, chains_per_lig, n_sample, orc=None):
         orc.set_receptor(xyz, xs)
         orc.set_box([0, 0, 0], [BOX] * 3)
         t_grid = orc.grid_seconds(synth.TYPES8, threads)
+    if warm is not None:
+        lw = orc.add_ligand(warm)
+        dw = max(1, int((0.24 * warm["n_atoms"] + 0.29 * orc.ntors[lw] - 3.41) * 2))
+        orc.mc_chains(lw, SEED, lw, dw, (30 + warm["n_atoms"]) // 3, 0, chains_per_lig, threads=threads)
     total_t, total_evals, desc = 0.0, 0, []
     for lig in ligs[:n_sample]:
         lo = orc.add_ligand(lig)
@@ -428,6 +454,7 @@ def run_ours(a):
     for _ in range(3):
         ctx.build_grids(synth.TYPES8)
         grid_ms.append(ctx.stats()["grid_ms"])
+    cells_ms = ctx.stats()["cells_ms"]
     n_pts = int(np.prod(ctx.grid_dims()[0]))
     grid_bytes = 4 * n_pts * 8 + 16 * REC_ATOMS
     ids = [ctx.add_ligand(l) for l in ligs]
@@ -505,7 +532,7 @@ def run_ours(a):
         "dock_kernel_evals_per_s": evals / (dock_ms / 1e3)}
     # end to end through the public API with host buffers: ligand topologies
     # copied in (vd_add_ligand + pool upload), results read back
-    e2e_times, h2d, d2h = [], 0, 0
+    e2e_times, h2d_steps = [], []
     n_e2e = K if a.e2e_steps <= 0 else min(a.e2e_steps, K)
     for k in range(n_e2e):
         torch.cuda.synchronize()
@@ -515,12 +542,10 @@ def run_ours(a):
         res = ctx.dock_batched(eids, sp)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    def blob_bytes(lig):  # the ligand's pool blob (ligand.cpp layout), uploaded once per call
-        heavy, nn, npairs = int((lig["xs"] >= 0).sum()), len(lig["node_parent"]), len(lig["pairs"])
-        lp_iters = ((npairs + 31) // 32 + 1) // 2
-        return 16 * (4 + heavy + 3 * nn + max(1, (npairs + 1) // 2) + max(1, 32 * lp_iters))
-    h2d = int(sum(blob_bytes(ligs[i]) for k in range(n_e2e) for i in batches[W + k]) / max(1, n_e2e))
-    d2h = B * 2 * 1024  # vd_dock_result per ligand
+        h2d_steps.append(ctx.stats()["ligand_bytes"])  # the batch's ligand blobs, uploaded by the call
+    h2d = int(sum(h2d_steps) / max(1, len(h2d_steps)))
+    import ctypes
+    d2h = B * ctypes.sizeof(vdock.DockResult)  # one vd_dock_result per ligand
     e2e_total = sum(e2e_times)
     if pg:
         e2e_total = multi.max_over_ranks(e2e_total, device="cuda")
@@ -540,12 +565,15 @@ def run_ours(a):
                    "l2": "inputs larger than L2 (8 maps x 188^3 x 4 B = 213 MB)",
                    "untimed_warmup_calls": n_warm, **shapes},
         "bfgs_evals_per_s": evals * world / elapsed,
+        "bfgs_evals_per_step": evals / K,
         "plain": {"value": plain_value * world, "unit": UNIT, "batched_over_plain": value / (plain_value * world),
                   **plain_split},
         "batched_split": batched_split,
         "grid_build": {"ms": min(grid_ms), "points": n_pts, "types": 8,
                        "gbs": grid_bytes / (min(grid_ms) / 1e3) / 1e9,
-                       "frac_of_hbm": grid_bytes / (min(grid_ms) / 1e3) / 1e9 / hbm},
+                       "frac_of_hbm": grid_bytes / (min(grid_ms) / 1e3) / 1e9 / hbm,
+                       "corner_cells_ms": cells_ms,
+                       **grid_l1_roof(min(grid_ms), clk, local)},
         "roofline": {"kernel": "dock_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": (DOCK_DRAM_BYTES_PER_EVAL[shapes["dock_launch_shape"]] * evals / K
@@ -557,8 +585,11 @@ def run_ours(a):
         "clocks": clk,
         "wall_s": t_wall,
     }
-    if world == 1 and not a.no_cpu_baseline:  # the reference arm's first timed step
-        cb = cpu_baseline(xyz, xs, ligs[W * B:W * B + a.cpu_ligands], a.chains, a.cpu_ligands)
+    if world == 1 and not a.no_cpu_baseline:
+        # the reference arm's sample of the first two timed steps (the first
+        # cpu_ligands ligands of each batch), after one untimed warm-up ligand
+        sample = [lig for k in range(W, min(W + 2, W + K)) for lig in ligs[k * B:k * B + a.cpu_ligands]]
+        cb = cpu_baseline(xyz, xs, sample, a.chains, len(sample), warm=ligs[0])
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         line["grid_build"]["cpu_s"] = cb["grid_build_s"]
     ctx.close()

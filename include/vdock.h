@@ -135,6 +135,9 @@ typedef struct {
                                     32-byte trilinear corner cells for the
                                     evaluation kernels (0 when the box is too
                                     large for them and the kernels read the maps) */
+    int64_t ligand_bytes;        /* device blobs of all ligands added since the
+                                    last vd_clear_ligands (what the ligand uploads
+                                    copy to the GPU)                            */
 } vd_stats;
 
 /* ---- context ------------------------------------------------------------ */

@@ -117,11 +117,14 @@ def _near_discontinuity(orc, lo, pose, n_atoms, pairs, grid):
 
 def test_adjoint_all_65536_poses(vd):
     """Every pose of the adjoint-check workload: energies within 1e-3
-    kcal/mol when every heavy atom lies at least 1e-3 A inside the box; else
-    within 1e-3 + 1e-5 |E| plus the out-of-box slope (1e6 kcal/mol/A) times
-    the summed coordinate difference of the atoms outside, GPU (FP32)
-    against oracle (FP64) -- the penalty turns coordinate rounding into
-    energy; gradients within 1e-3 of max(1, |g_ref|_inf).
+    kcal/mol when every heavy atom lies at least 1e-3 A inside the box.
+    Outside it the penalty (grid.cpp:50-160: slope 1e6 kcal/mol/A times the
+    distance beyond the box) turns FP32 rounding into energy, so the bound is
+    1e-3 + 1e-5 |E| (FP32 sums) plus the slope times, per atom and axis
+    outside the box, the GPU-oracle coordinate difference and four FP32 ulps
+    each of the coordinate and of the atom's box coordinate s in cells (the
+    distance beyond the far face, s - (n - 1), cancels in FP32: one ulp at
+    s = 107 is 7.6e-6 cells, 2.9 kcal/mol).  Gradients within 1e-3 of max(1, |g_ref|_inf).
 
     A gradient outside that bound is accepted only at a discontinuity of the
     reference's gradient (an atom on a grid-cell face or a pair at the cutoff,
@@ -150,7 +153,8 @@ def test_adjoint_all_65536_poses(vd):
     e_gpu, g_gpu = ctx.energy_grad(lc, poses)
     x = ctx.pose_coords(lc, poses)
     grid = orc.grid_info()
-    _, b, e = grid
+    npts, b, e = grid
+    cell = (e - b) / (npts - 1)
     inside = np.all((x >= b + 1e-3) & (x <= e - 1e-3), axis=(1, 2))
     assert inside.sum() >= n // 2, inside.sum()
     pairs = np.asarray(lig["pairs"]).reshape(-1, 2)
@@ -165,8 +169,11 @@ def test_adjoint_all_65536_poses(vd):
         tol = E_TOL
         if not inside[i]:
             xr = orc.coords(lo, c, lig["n_atoms"])[heavy]
-            out = np.any((xr < b) | (xr > e) | (x[i] < b) | (x[i] > e), axis=1)
-            tol = E_TOL + 1e-5 * abs(er) + 1e6 * float(np.abs(x[i][out] - xr[out]).sum())
+            out = (xr < b) | (xr > e) | (x[i] < b) | (x[i] > e)  # [atom][axis]
+            s_cells = np.abs((x[i].astype(np.float64) - b) / cell)
+            ulps = (np.spacing(s_cells.astype(np.float32)).astype(np.float64) * cell +
+                    np.spacing(np.abs(x[i])).astype(np.float64))
+            tol = E_TOL + 1e-5 * abs(er) + 1e6 * float((np.abs(x[i] - xr) + 4 * ulps)[out].sum())
         assert de <= tol, (i, e_gpu[i], er, tol)
         gscale = max(1.0, np.abs(gr).max())
         dg = np.abs(g_gpu[i] - gr).max() / gscale
@@ -180,7 +187,7 @@ def test_adjoint_all_65536_poses(vd):
         elif inside[i]:
             worst_e, worst_g = max(worst_e, de), max(worst_g, dg)
     assert len(outliers) <= n // 1000, outliers
-    idx = np.flatnonzero(inside)[::256]
+    idx = [i for i in np.flatnonzero(inside)[::256] if i not in outliers]  # outliers sit on a discontinuity
     n_ok = n_tot = 0
     for i in idx:
         c = poses[i].astype(np.float64)

@@ -306,3 +306,30 @@ def test_parser_survives_mutated_inputs(lib, golden_dir):
         assert st in (0, 5), st
         seen[st] += 1
     assert seen[0] > 100 and seen[5] > 100
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """The Python mirror's structs (vdock.SearchParams, Stats, DockResult,
+    LigandDesc, EvalParams) have the sizes and field offsets of the C
+    declarations in include/vdock.h, compiled here with the host C compiler."""
+    import ctypes as C
+    import subprocess
+    import vdock
+    structs = {"vd_search_params": vdock.SearchParams, "vd_stats": vdock.Stats, "vd_dock_result": vdock.DockResult,
+               "vd_ligand_desc": vdock.LigandDesc, "vd_eval_params": vdock.EvalParams}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "vdock.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in py._fields_:
+            lines.append(f'printf("{cname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "abi.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "abi"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f in py._fields_:
+            assert got[(cname, f[0])] == getattr(py, f[0]).offset, (cname, f[0])

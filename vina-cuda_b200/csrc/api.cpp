@@ -149,6 +149,7 @@ vd_status vd_get_stats(vd_ctx* h, vd_stats* out) {
     VD_CHECK(h && out, VD_ERR_ARG, "vd_get_stats: NULL argument");
     h->c.stats.device_bytes = int64_t(h->c.dev_used);
     h->c.stats.pair_force_scale = h->c.fix_scale;
+    h->c.stats.ligand_bytes = h->c.pool_words * int64_t(sizeof(float4));
     *out = h->c.stats;
     return VD_OK;
 }

@@ -6,17 +6,19 @@
 //        q_k = q_root * aa_j1 * ... * aa_k,  o_k = o_root + R_root * w_k
 //      (rotation about a body-fixed axis; equals tree.h:282-292)
 //   3. lanes = atoms: coordinates, trilinear grid term (grid.cpp:50-160)
-//   4. lanes = segments of the pair list sorted by second atom, two pairs
-//      per iteration (read from the lane-interleaved copy): intra pair term;
-//      the force on the first atom is added with a shared-memory atomic, the
-//      force on the second atom either summed in registers while the atom
-//      repeats or, in the search (pair_atomics), added with an atomic too
-//      (model.cpp:1241-1256).  Pair forces are summed in 32-bit fixed point
-//      (EvalParams::fix units per kcal/mol/A, set from the tables so that
-//      no atom's sum can overflow): on B200 shared-memory 32-bit integer
-//      atomics cost the same however many lanes hit one atom, FP32 (and
-//      64-bit) ones serialise those lanes; integer sums are exact, so the
-//      result does not depend on the order in which the atomics land
+//   4. intra pair term (model.cpp:1241-1256), two pairs per lane per
+//      iteration.  The search (pair_atomics) walks the ligand's search
+//      schedule: rounds of one pair per lane in which few lanes share an
+//      atom, both atoms' forces added with shared-memory atomics.  The pose
+//      kernels walk per-lane segments of the pair list sorted by second atom,
+//      the second atom's force summed in registers while it repeats, the
+//      first atom's added with an atomic.  Pair forces are summed in 32-bit
+//      fixed point (EvalParams::fix units per kcal/mol/A, set from the tables
+//      so that no atom's sum can overflow): integer sums are exact, so the
+//      result does not depend on the order in which the atomics land, and
+//      32-bit integer shared atomics are the cheapest kind on B200 (FP32 and
+//      64-bit ones cost more per lane); atomics of several lanes of one
+//      instruction to the same address serialise, which the schedule avoids
 //   6. lanes = contiguous atom ranges: warp prefix sums over the heavy atoms
 //      of force and moment about the root origin
 //   7. lanes = bodies: subtree sums as differences of two prefixes (a
@@ -52,7 +54,9 @@ struct LigView {
     const NodeRec* nodes;
     const int2* pairs;
     const int4* lpairs;         // per-lane segments, two pairs per entry, interleaved by lane
+    const int4* spairs;         // search schedule: rounds of one pair per lane, two rounds per entry
     int32_t na, nn, np, nt;
+    int32_t sp_iters;           // schedule entries per lane
     float num_tors;
 };
 
@@ -69,6 +73,8 @@ __device__ __forceinline__ LigView lig_view(const float4* pool, int64_t off) {
     L.nodes = reinterpret_cast<const NodeRec*>(b + h->off_nodes);
     L.pairs = reinterpret_cast<const int2*>(b + h->off_pairs);
     L.lpairs = reinterpret_cast<const int4*>(b + h->off_lpairs);
+    L.spairs = reinterpret_cast<const int4*>(b + h->off_spairs);
+    L.sp_iters = h->sp_iters;
     return L;
 }
 
@@ -298,11 +304,12 @@ struct GridInter {
     }
 };
 
-// pair_atomics: the force on a pair's second atom also goes straight to its
-// accumulator with an atomic instead of being summed in registers along the
-// segment.  That is shorter and less divergent code, which the latency-bound
-// search prefers (+3-5%); the pose kernels, bound by L1 wavefronts, keep the
-// register sums (fewer atomics and coordinate loads, +14% there).
+// pair_atomics: pairs from the search schedule, both atoms' forces by
+// atomics (no per-lane flush when the second atom changes: shorter, less
+// divergent code, which the latency-bound search prefers); otherwise the
+// second atom's force is summed in registers along b-sorted segments, which
+// the pose kernels, bound by L1 wavefronts, prefer (fewer atomics and
+// coordinate loads).
 template <bool want_grad, bool pair_atomics = false, class Inter>
 __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const Inter& inter, const float4* smooth,
                              float v_intra, float fix, float inv_fix, int lane) {
@@ -322,13 +329,64 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         }
     }
     if (want_grad) __syncwarp();
-    // 4: intra pairs.  Pairs are sorted by their second atom b; each lane
-    // takes a contiguous segment, two pairs at a time (two table gathers in
-    // flight), keeps b's coordinates and force in registers while b repeats
-    // (unless pair_atomics), and adds the force on a with an atomic.  Table
-    // indices are clamped and pairs past the cutoff masked (their table
-    // loads predicated off).
-    {
+    // 4: intra pairs, two per lane per iteration (two table gathers in
+    // flight); table indices are clamped and pairs past the cutoff masked
+    // (their table loads predicated off).
+    //  - pair_atomics (the search): the ligand's search schedule, one pair per
+    //    lane per round; both atoms' forces go to their accumulators with
+    //    atomics, and the rounds are built so few lanes share an atom;
+    //  - otherwise: pairs sorted by their second atom b, each lane a
+    //    contiguous segment, b's coordinates and force kept in registers
+    //    while b repeats, the force on a added with an atomic.
+    if (pair_atomics) {
+        int* const qx = reinterpret_cast<int*>(m.ns);
+        int* const qy = qx + pad4(L.na);
+        int* const qz = qy + pad4(L.na);
+        const int4* sp = L.spairs + lane;
+        for (int k = 0; k < L.sp_iters; ++k, sp += 32) {
+            const int4 qq = __ldg(sp);  // coalesced across the warp
+            const bool v0 = qq.y >= 0, v1 = qq.w >= 0;  // unused slots carry type pair -1
+            const int a0 = VD_DCLAMP(qq.x & 0xffff, 0, L.na - 1, kChkPairAtom);
+            const int b0 = VD_DCLAMP(qq.x >> 16, 0, L.na - 1, kChkPairAtom);
+            const int a1 = VD_DCLAMP(qq.z & 0xffff, 0, L.na - 1, kChkPairAtom);
+            const int b1 = VD_DCLAMP(qq.z >> 16, 0, L.na - 1, kChkPairAtom);
+            const float4 ca0 = m.c[a0], cb0 = m.c[b0], ca1 = m.c[a1], cb1 = m.c[b1];
+            const float r0x = cb0.x - ca0.x, r0y = cb0.y - ca0.y, r0z = cb0.z - ca0.z;
+            const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
+            const float d0 = r0x * r0x + r0y * r0y + r0z * r0z, d1 = r1x * r1x + r1y * r1y + r1z * r1z;
+            const float rf0 = fminf(32.f * d0, 2047.5f), rf1 = fminf(32.f * d1, 2047.5f);
+            const int i0 = VD_DCLAMP(int(rf0), 0, kBins - 2, kChkTableBin);
+            const int i1 = VD_DCLAMP(int(rf1), 0, kBins - 2, kChkTableBin);
+            const int tp0 = VD_DCLAMP(v0 ? qq.y : 0, 0, kPairTypes - 1, kChkPairType);
+            const int tp1 = VD_DCLAMP(v1 ? qq.w : 0, 0, kPairTypes - 1, kChkPairType);
+            const bool in0 = v0 && d0 < 64.f, in1 = v1 && d1 < 64.f;
+            float4 t0 = make_float4(0.f, 0.f, 0.f, 0.f), t1 = t0;
+            if (in0) t0 = __ldg(smooth + size_t(tp0) * kBins + i0);  // no gather past the cutoff
+            if (in1) t1 = __ldg(smooth + size_t(tp1) * kBins + i1);
+            const float w0 = rf0 - float(i0), w1 = rf1 - float(i1);
+            float e0 = t0.x + w0 * (t0.z - t0.x), g0 = t0.y + w0 * (t0.w - t0.y);
+            float e1 = t1.x + w1 * (t1.z - t1.x), g1 = t1.y + w1 * (t1.w - t1.y);
+            const float c0 = (e0 > 0.f) ? __fdividef(v_intra, v_intra + e0) : 1.f;
+            const float c1 = (e1 > 0.f) ? __fdividef(v_intra, v_intra + e1) : 1.f;
+            e0 = in0 ? e0 * c0 : 0.f;
+            e1 = in1 ? e1 * c1 : 0.f;
+            e += e0 + e1;
+            if (want_grad) {
+                // fixed point: fix is a power of two, so (g * fix) * r rounds exactly like (g * r) * fix
+                const float gf0 = in0 ? g0 * c0 * c0 * fix : 0.f, gf1 = in1 ? g1 * c1 * c1 * fix : 0.f;
+                if (in0) {
+                    const int Fx = __float2int_rn(gf0 * r0x), Fy = __float2int_rn(gf0 * r0y), Fz = __float2int_rn(gf0 * r0z);
+                    atomicAdd(&qx[a0], -Fx); atomicAdd(&qy[a0], -Fy); atomicAdd(&qz[a0], -Fz);
+                    atomicAdd(&qx[b0], Fx); atomicAdd(&qy[b0], Fy); atomicAdd(&qz[b0], Fz);
+                }
+                if (in1) {
+                    const int Fx = __float2int_rn(gf1 * r1x), Fy = __float2int_rn(gf1 * r1y), Fz = __float2int_rn(gf1 * r1z);
+                    atomicAdd(&qx[a1], -Fx); atomicAdd(&qy[a1], -Fy); atomicAdd(&qz[a1], -Fz);
+                    atomicAdd(&qx[b1], Fx); atomicAdd(&qy[b1], Fy); atomicAdd(&qz[b1], Fz);
+                }
+            }
+        }
+    } else {
         const int len = (((lane + 1) * L.np) >> 5) - ((lane * L.np) >> 5);
         const int4* lp = L.lpairs + lane;
         int cur_b = -1;
@@ -354,11 +412,11 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const int b0 = VD_DCLAMP(q0.x >> 16, 0, L.na - 1, kChkPairAtom);
             const int a1 = VD_DCLAMP(q1.x & 0xffff, 0, L.na - 1, kChkPairAtom);
             const int b1 = VD_DCLAMP(q1.x >> 16, 0, L.na - 1, kChkPairAtom);
-            if (!pair_atomics && b0 != cur_b) {  // b repeats along the segment: its coordinates stay in registers
+            if (b0 != cur_b) {  // b repeats along the segment: its coordinates stay in registers
                 flush(b0);
                 cb = m.c[b0];
             }
-            const float4 cb0 = pair_atomics ? m.c[b0] : cb, cb1 = (pair_atomics || b1 != b0) ? m.c[b1] : cb;
+            const float4 cb0 = cb, cb1 = (b1 != b0) ? m.c[b1] : cb;
             const float4 ca0 = m.c[a0], ca1 = m.c[a1];
             const float r0x = cb0.x - ca0.x, r0y = cb0.y - ca0.y, r0z = cb0.z - ca0.z;
             const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
@@ -382,22 +440,11 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             g0 = in0 ? g0 * c0 * c0 : 0.f;
             g1 = in1 ? g1 * c1 * c1 : 0.f;
             e += e0 + e1;
-            if (!pair_atomics && !want_grad && two && b1 != cur_b) {
+            if (!want_grad && two && b1 != cur_b) {
                 cur_b = b1;
                 cb = cb1;
             }
-            if (want_grad && pair_atomics) {
-                if (in0) {
-                    const int Fx = to_fixed(g0 * r0x, fix), Fy = to_fixed(g0 * r0y, fix), Fz = to_fixed(g0 * r0z, fix);
-                    atomicAdd(&qx[a0], -Fx); atomicAdd(&qy[a0], -Fy); atomicAdd(&qz[a0], -Fz);
-                    atomicAdd(&qx[b0], Fx); atomicAdd(&qy[b0], Fy); atomicAdd(&qz[b0], Fz);
-                }
-                if (in1) {
-                    const int Fx = to_fixed(g1 * r1x, fix), Fy = to_fixed(g1 * r1y, fix), Fz = to_fixed(g1 * r1z, fix);
-                    atomicAdd(&qx[a1], -Fx); atomicAdd(&qy[a1], -Fy); atomicAdd(&qz[a1], -Fz);
-                    atomicAdd(&qx[b1], Fx); atomicAdd(&qy[b1], Fy); atomicAdd(&qz[b1], Fz);
-                }
-            } else if (want_grad) {
+            if (want_grad) {
                 if (in0) {
                     const float Fx = g0 * r0x, Fy = g0 * r0y, Fz = g0 * r0z;
                     atomicAdd(&qx[a0], to_fixed(-Fx, fix)); atomicAdd(&qy[a0], to_fixed(-Fy, fix));

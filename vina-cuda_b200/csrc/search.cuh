@@ -114,82 +114,101 @@ struct SearchMem {  // per-warp shared memory of the optimiser
 // quasi_newton.cuh:2172-2389 (RILC-BFGS) with the Lewis-Overton line search
 // of quasi_newton.cuh:1710-1806, on the pose in s.m.x.  Returns the energy;
 // s.m.x holds the optimised pose.  *evals counts energy+gradient calls.
+//
+// The loop has one evaluation site: the entry evaluation and every
+// line-search trial run through the same inlined copy of the evaluation
+// (about 30 KB of code), so the search kernel's hot code fits the
+// instruction caches better.  The operations and their order are those of
+// the straight-line form: entry evaluation, then per iteration a line search
+// (start, trials) and the direction update.
 __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const MapView& G, const float4* smooth,
                            const EvalParams ep, int max_steps, int lane, int& evals) {
     const int n = 6 + L.nt, nc = 7 + L.nt;
     if (max_steps <= 0) max_steps = 1000;  // the reference's 0 means unbounded
-    float fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane);
-    ++evals;
-    Vec2 g = vload(s.m.g, n, lane);
-    const float fx_orig = fx;
-    copy_conf(s.m.x, s.xo, nc, lane);
-    Vec2 d = {-g.a, -g.b};
-    const float gg = vdot(g, g);  // = d.d (d = -g)
-    if (!(sqrtf(gg) >= 1e-5f)) return fx;
-    float step = 1.f / sqrtf(gg);
-    int k = 1;
+    float fx = 0.f, fx_orig = 0.f, fxp = 0.f, step = 0.f;
+    Vec2 g = {0.f, 0.f}, gp = {0.f, 0.f}, d = {0.f, 0.f};
+    // line-search state
+    int count = 0, k = 1;
+    bool brackt = false, first = true;
+    float mu = 0.f, nu = 1.0e20f, finit = 0.f, dgtest = 0.f, dstest = 0.f;
     for (;;) {
-        copy_conf(s.m.x, s.xp, nc, lane);
-        const Vec2 gp = g;
-        const float fxp = fx;
-        // ---- line search
-        int ls;
-        {
-            int count = 0;
-            bool brackt = false;
-            float mu = 0.f, nu = 1.0e20f;
-            const float dginit = vdot(gp, d);
-            if (0.f < dginit) {
-                ls = -1;
+        if (!first) conf_step(s.xp, s.m.x, d, step, L.nt, lane);  // the line search's trial pose
+        fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane);
+        ++evals;
+        g = vload(s.m.g, n, lane);
+        if (first) {
+            first = false;
+            fx_orig = fx;
+            copy_conf(s.m.x, s.xo, nc, lane);
+            d = Vec2{-g.a, -g.b};
+            const float gg = vdot(g, g);  // = d.d (d = -g)
+            if (!(sqrtf(gg) >= 1e-5f)) return fx;
+            step = 1.f / sqrtf(gg);
+        } else {
+            ++count;
+            bool accept = false;
+            if (fx > finit + step * dgtest) {
+                nu = step;
+                brackt = true;
             } else {
-                const float finit = fx, dgtest = 1.0e-4f * dginit, dstest = 0.1f * dginit;
-                for (;;) {
-                    conf_step(s.xp, s.m.x, d, step, L.nt, lane);
-                    fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane);
-                    ++evals;
-                    g = vload(s.m.g, n, lane);
-                    ++count;
-                    if (fx > finit + step * dgtest) {
-                        nu = step;
-                        brackt = true;
-                    } else {
-                        if (vdot(g, d) < dstest) mu = step;
-                        else { ls = count; break; }
-                    }
-                    if (count >= 10) { ls = (fx > finit) ? -1 : count; break; }
-                    step = brackt ? 0.5f * (mu + nu) : 2.f * step;
-                }
+                if (vdot(g, d) < dstest) mu = step;
+                else accept = true;
             }
+            if (!accept && count >= 10) {
+                if (fx > finit) {  // the line search failed: back to its start
+                    copy_conf(s.xp, s.m.x, nc, lane);
+                    g = gp;
+                    fx = fxp;
+                    break;
+                }
+                accept = true;
+            }
+            if (!accept) {
+                step = brackt ? 0.5f * (mu + nu) : 2.f * step;
+                continue;
+            }
+            // the update's dot products that do not depend on one another, in one
+            // reduction: g.g, y.s, y.y, s.s, gp.gp and s.d with d = -g
+            const Vec2 sv = {step * d.a, step * d.b};
+            const Vec2 yv = {g.a - gp.a, g.b - gp.b};
+            const Vec2 dn = {-g.a, -g.b};
+            float dots[6] = {lane_dot(g, g), lane_dot(yv, sv), lane_dot(yv, yv), lane_dot(sv, sv), lane_dot(gp, gp),
+                             lane_dot(sv, dn)};
+            warp_sum_n(dots);
+            if (!(sqrtf(dots[0]) >= 1e-5f)) return fx;
+            if (max_steps <= k) break;
+            ++k;
+            const float ys = dots[1], yy = dots[2];
+            d = dn;
+            const float cau = dots[3] * sqrtf(dots[4]) * 1.0e-6f;
+            if (ys > cau) {
+                const float alpha = dots[5] / ys;
+                d.a += alpha * yv.a; d.b += alpha * yv.b;
+                const float sc = ys / yy;
+                d.a *= sc; d.b *= sc;
+                const float beta = vdot(yv, d) / ys;
+                d.a += (alpha - beta) * sv.a; d.b += (alpha - beta) * sv.b;
+            }
+            step = 1.f;
         }
-        if (ls < 0) {
+        // start a line search from the current pose
+        copy_conf(s.m.x, s.xp, nc, lane);
+        gp = g;
+        fxp = fx;
+        count = 0;
+        brackt = false;
+        mu = 0.f;
+        nu = 1.0e20f;
+        const float dginit = vdot(gp, d);
+        if (0.f < dginit) {  // not a descent direction
             copy_conf(s.xp, s.m.x, nc, lane);
             g = gp;
             fx = fxp;
             break;
         }
-        // the update's dot products that do not depend on one another, in one
-        // reduction: g.g, y.s, y.y, s.s, gp.gp and s.d with d = -g
-        const Vec2 sv = {step * d.a, step * d.b};
-        const Vec2 yv = {g.a - gp.a, g.b - gp.b};
-        const Vec2 dn = {-g.a, -g.b};
-        float dots[6] = {lane_dot(g, g), lane_dot(yv, sv), lane_dot(yv, yv), lane_dot(sv, sv), lane_dot(gp, gp),
-                         lane_dot(sv, dn)};
-        warp_sum_n(dots);
-        if (!(sqrtf(dots[0]) >= 1e-5f)) return fx;
-        if (max_steps <= k) break;
-        ++k;
-        const float ys = dots[1], yy = dots[2];
-        d = dn;
-        const float cau = dots[3] * sqrtf(dots[4]) * 1.0e-6f;
-        if (ys > cau) {
-            const float alpha = dots[5] / ys;
-            d.a += alpha * yv.a; d.b += alpha * yv.b;
-            const float sc = ys / yy;
-            d.a *= sc; d.b *= sc;
-            const float beta = vdot(yv, d) / ys;
-            d.a += (alpha - beta) * sv.a; d.b += (alpha - beta) * sv.b;
-        }
-        step = 1.f;
+        finit = fx;
+        dgtest = 1.0e-4f * dginit;
+        dstest = 0.1f * dginit;
     }
     if (!(fx <= fx_orig)) {
         fx = fx_orig;
@@ -211,12 +230,64 @@ __device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, floa
                            float inv_fix, int max_steps, int lane, int& evals) {
     const int n = 6 + L.nt, nc = 7 + L.nt;
     for (int i = lane; i < n * n; i += 32) H[i] = (i / n == i % n) ? 1.f : 0.f;
-    float f0 = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
-    ++evals;
-    for (int i = lane; i < n; i += 32) gc[i] = s.m.g[i];
-    const float f_orig = f0;
-    copy_conf(s.m.x, s.xo, nc, lane);
-    for (int step = 0; step < max_steps; ++step) {
+    // One evaluation site (the entry evaluation and every line-search trial),
+    // as in rilc_bfgs; the operations and their order are the straight-line
+    // algorithm's.  As in the reference's line search, a trial that fails
+    // the Armijo test halves alpha, the tenth failure included, and the step
+    // keeps the last trial pose.
+    float f0 = 0.f, f_orig = 0.f, alpha = 1.f, pg = 0.f;
+    Vec2 p = {0.f, 0.f}, g = {0.f, 0.f};
+    int step = 0, trial = 0;
+    bool first = true;
+    for (;;) {
+        if (!first) conf_step(s.xp, s.m.x, p, alpha, L.nt, lane);
+        const float fe = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
+        ++evals;
+        if (first) {
+            first = false;
+            f0 = fe;
+            for (int i = lane; i < n; i += 32) gc[i] = s.m.g[i];
+            f_orig = f0;
+            copy_conf(s.m.x, s.xo, nc, lane);
+        } else {
+            if (!(fe - f0 < 0.0001f * alpha * pg)) {  // line_search, bfgs.h:65-82
+                alpha *= 0.5f;
+                if (++trial < 10) continue;
+            }
+            const Vec2 gn = vload(s.m.g, n, lane);
+            const Vec2 y = {gn.a - g.a, gn.b - g.b};
+            f0 = fe;
+            if (!(sqrtf(vdot(g, g)) >= 1e-5f)) break;
+            for (int i = lane; i < n; i += 32) { gc[i] = s.m.g[i]; yv[i] = s.m.g[i] - (i < 32 ? g.a : g.b); }
+            __syncwarp();
+            if (step == 0) {
+                const float yy = vdot(y, y);
+                if (fabsf(yy) > FLT_EPSILON) {
+                    const float dg = alpha * vdot(y, p) / yy;
+                    for (int i = lane; i < n; i += 32) H[i * n + i] = dg;
+                    __syncwarp();
+                }
+            }
+            const float yp = vdot(y, p);  // bfgs_update, bfgs.h:49-63
+            if (!(alpha * yp < FLT_EPSILON)) {
+                for (int i = lane; i < n; i += 32) {
+                    float sum = 0.f;
+                    for (int j = 0; j < n; ++j) sum += H[i * n + j] * yv[j];
+                    mhy[i] = -sum;
+                }
+                __syncwarp();
+                const float yhy = -vdot(y, vload(mhy, n, lane));
+                const float r = 1.f / (alpha * yp);
+                const float c2 = alpha * alpha * (r * r * yhy + r);
+                for (int idx = lane; idx < n * n; idx += 32) {
+                    const int i = idx / n, j = idx % n;
+                    H[idx] += alpha * r * (mhy[i] * pv[j] + mhy[j] * pv[i]) + c2 * pv[i] * pv[j];
+                }
+                __syncwarp();
+            }
+            ++step;
+        }
+        if (step >= max_steps) break;
         for (int i = lane; i < n; i += 32) {  // p = -H g
             float sum = 0.f;
             for (int j = 0; j < n; ++j) sum += H[i * n + j] * gc[j];
@@ -224,46 +295,11 @@ __device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, floa
         }
         __syncwarp();
         copy_conf(s.m.x, s.xp, nc, lane);
-        const Vec2 p = vload(pv, n, lane), g = vload(gc, n, lane);
-        const float pg = vdot(p, g);
-        float alpha = 1.f, f1 = 0.f;
-        for (int trial = 0; trial < 10; ++trial) {  // line_search, bfgs.h:65-82
-            conf_step(s.xp, s.m.x, p, alpha, L.nt, lane);
-            f1 = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
-            ++evals;
-            if (f1 - f0 < 0.0001f * alpha * pg) break;
-            alpha *= 0.5f;
-        }
-        const Vec2 gn = vload(s.m.g, n, lane);
-        const Vec2 y = {gn.a - g.a, gn.b - g.b};
-        f0 = f1;
-        if (!(sqrtf(vdot(g, g)) >= 1e-5f)) break;
-        for (int i = lane; i < n; i += 32) { gc[i] = s.m.g[i]; yv[i] = s.m.g[i] - (i < 32 ? g.a : g.b); }
-        __syncwarp();
-        if (step == 0) {
-            const float yy = vdot(y, y);
-            if (fabsf(yy) > FLT_EPSILON) {
-                const float dg = alpha * vdot(y, p) / yy;
-                for (int i = lane; i < n; i += 32) H[i * n + i] = dg;
-                __syncwarp();
-            }
-        }
-        const float yp = vdot(y, p);  // bfgs_update, bfgs.h:49-63
-        if (alpha * yp < FLT_EPSILON) continue;
-        for (int i = lane; i < n; i += 32) {
-            float sum = 0.f;
-            for (int j = 0; j < n; ++j) sum += H[i * n + j] * yv[j];
-            mhy[i] = -sum;
-        }
-        __syncwarp();
-        const float yhy = -vdot(y, vload(mhy, n, lane));
-        const float r = 1.f / (alpha * yp);
-        const float c2 = alpha * alpha * (r * r * yhy + r);
-        for (int idx = lane; idx < n * n; idx += 32) {
-            const int i = idx / n, j = idx % n;
-            H[idx] += alpha * r * (mhy[i] * pv[j] + mhy[j] * pv[i]) + c2 * pv[i] * pv[j];
-        }
-        __syncwarp();
+        p = vload(pv, n, lane);
+        g = vload(gc, n, lane);
+        pg = vdot(p, g);
+        alpha = 1.f;
+        trial = 0;
     }
     if (!(f0 <= f_orig)) {
         f0 = f_orig;

@@ -57,7 +57,7 @@ class Stats(C.Structure):
                 ("post_ms", C.c_double), ("dock_warps_per_block", C.c_int32), ("dock_blocks", C.c_int32),
                 ("dock_shape", C.c_int32), ("grid_shape", C.c_int32), ("graph_launches", C.c_int64),
                 ("graph_instantiations", C.c_int64), ("scoring_ms", C.c_double), ("device_bytes", C.c_int64),
-                ("pair_force_scale", C.c_double), ("cells_ms", C.c_double)]
+                ("pair_force_scale", C.c_double), ("cells_ms", C.c_double), ("ligand_bytes", C.c_int64)]
 
 
 EXPORTS = [
