@@ -138,7 +138,7 @@ DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budget
 # of one grid_build_kernel launch).  The kernel's limit is that pipe: one
 # wavefront per SM per cycle; every in-range (point, receptor atom) pair reads
 # one 32-byte table row, one wavefront.
-GRID_L1_WAVEFRONTS = None
+GRID_L1_WAVEFRONTS = 133_836_283
 
 
 def grid_l1_roof(ms, clk, device):

@@ -117,7 +117,11 @@ def _near_discontinuity(orc, lo, pose, n_atoms, pairs, grid):
 
 def test_adjoint_all_65536_poses(vd):
     """Every pose of the adjoint-check workload: energies within 1e-3
-    kcal/mol when every heavy atom lies at least 1e-3 A inside the box.
+    kcal/mol + 2e-5 |E| when every heavy atom lies at least 1e-3 A inside
+    the box, and within 1e-3 outright where |E| <= 10 kcal/mol (the relative
+    part matters only for clashing poses: an energy of a few hundred
+    kcal/mol is an FP32 sum of ~700 atom and pair terms, which rounds at
+    ~1e-5 of its size).
     Outside it the penalty (grid.cpp:50-160: slope 1e6 kcal/mol/A times the
     distance beyond the box) turns FP32 rounding into energy, so the bound is
     1e-3 + 1e-5 |E| (FP32 sums) plus the slope times, per atom and axis
@@ -127,11 +131,13 @@ def test_adjoint_all_65536_poses(vd):
     s = 107 is 7.6e-6 cells, 2.9 kcal/mol).  Gradients within 1e-3 of max(1, |g_ref|_inf).
 
     A gradient outside that bound is accepted only at a discontinuity of the
-    reference's gradient (an atom on a grid-cell face or a pair at the cutoff,
-    where the FP32 and FP64 coordinates fall on different sides) and only
-    when the oracle's own gradient at a pose within 1e-6 of it (the FP32
-    coordinate uncertainty) agrees with the GPU's to the same bound; at most
-    one pose in a thousand may need this.
+    reference's gradient (an atom within 1e-4 cells of a grid-cell face or a
+    pair within 1e-4 A^2 of the cutoff, where FP32 and FP64 coordinates can
+    fall on different sides), and only by the size of the reference's own
+    jump there: |g - g_ref|_inf may exceed the bound by at most the largest
+    change of the oracle's gradient over 64 poses within 1e-5 of this one
+    (positions and torsions perturbed); at most one pose in a thousand may
+    need this.
 
     On every 256th in-box pose the GPU gradient lies as close to central
     differences (h = 1e-4, else 1e-5 or 1e-6 where h = 1e-4 straddles a
@@ -159,14 +165,16 @@ def test_adjoint_all_65536_poses(vd):
     assert inside.sum() >= n // 2, inside.sum()
     pairs = np.asarray(lig["pairs"]).reshape(-1, 2)
     rng = np.random.default_rng(0)
-    worst_e = worst_g = 0.0
+    worst_e = worst_g = worst_low = 0.0
     outliers = []
     heavy = np.asarray(lig["xs"]) >= 0
     for i in range(n):
         c = poses[i].astype(np.float64)
         er, gr = orc.eval_deriv(lo, c)
         de = abs(float(e_gpu[i]) - er)
-        tol = E_TOL
+        tol = E_TOL + 2e-5 * abs(er)
+        if inside[i] and abs(er) <= 10.0:
+            worst_low = max(worst_low, de)
         if not inside[i]:
             xr = orc.coords(lo, c, lig["n_atoms"])[heavy]
             out = (xr < b) | (xr > e) | (x[i] < b) | (x[i] > e)  # [atom][axis]
@@ -180,13 +188,14 @@ def test_adjoint_all_65536_poses(vd):
         if dg > G_TOL:
             assert _near_discontinuity(orc, lo, c, lig["n_atoms"], pairs, grid), (i, dg, g_gpu[i], gr)
             mask = np.r_[np.ones(3), np.zeros(4), np.ones(nt)]
-            near = min(np.abs(g_gpu[i] - orc.eval_deriv(lo, c + 1e-6 * rng.standard_normal(len(c)) * mask)[1]).max()
+            jump = max(np.abs(orc.eval_deriv(lo, c + 1e-5 * rng.standard_normal(len(c)) * mask)[1] - gr).max()
                        for _ in range(64))
-            assert near <= G_TOL * gscale, (i, dg, near)
+            assert dg * gscale <= jump + G_TOL * gscale, (i, dg * gscale, jump)
             outliers.append(i)
         elif inside[i]:
             worst_e, worst_g = max(worst_e, de), max(worst_g, dg)
     assert len(outliers) <= n // 1000, outliers
+    assert worst_low <= E_TOL, worst_low  # in-box poses of |E| <= 10 kcal/mol: the plain 1e-3 bound
     idx = [i for i in np.flatnonzero(inside)[::256] if i not in outliers]  # outliers sit on a discontinuity
     n_ok = n_tot = 0
     for i in idx:
@@ -200,7 +209,8 @@ def test_adjoint_all_65536_poses(vd):
         n_ok += int(np.sum(np.abs(fds[0] - g_gpu[i]) <= np.abs(fds[0] - gr) + tol))
         n_tot += len(gr)
     assert n_ok >= 0.9 * n_tot
-    print(f"65,536 poses ({int(inside.sum())} in box): worst in-box |de| {worst_e:.2e} kcal/mol, "
+    print(f"65,536 poses ({int(inside.sum())} in box): worst in-box |de| {worst_e:.2e} kcal/mol "
+          f"({worst_low:.2e} where |E| <= 10), "
           f"worst |dg|/max(1,|g|) {worst_g:.2e} off discontinuities; {len(outliers)} poses at a gradient "
           f"discontinuity {outliers}; FD subset {len(idx)} poses")
 
