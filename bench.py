@@ -125,12 +125,10 @@ def lig_bytes(lig):
 
 # DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
 # captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
-# ligands x 6,500 chains, 11.55 M evaluations per launch): 64 registers
-# 5.77 GB, 80 registers 4.52 GB, 128 registers 3.88 GB (the difference is
-# register spills).  The 48- and 40-register shapes, which the autotuner no
-# longer runs, were not captured with this kernel.  The bench scales the
-# figure by the evaluations of each launch.
-DOCK_DRAM_BYTES_PER_EVAL = {1: 499.0, 4: 392.0, 5: 336.0}
+# ligands x 6,500 chains, 11.55 M evaluations per launch): 80 registers
+# 5.60 GB per launch.  The bench scales the figure by the evaluations of
+# each launch; shapes not captured report no traffic.
+DOCK_DRAM_BYTES_PER_EVAL = {4: 485.0}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 # L1 data-pipe (LSU) wavefronts of one grid build of this workload (188^3
 # points x 8 maps, 8,000-atom receptor), from the ncu capture summarised in
@@ -475,8 +473,11 @@ def run_ours(a):
     ev0.record()
     dock_ms, post_ms, evals, abytes, launches = 0.0, 0.0, 0, 0, 0
     t_wall = time.perf_counter()
+    step_wall = []
     for k in range(W, W + K):
+        t_step = time.perf_counter()
         res = ctx.dock_batched(batches[k], sp)
+        step_wall.append(time.perf_counter() - t_step)  # the call returns after its GPU work
         st = ctx.stats()
         shapes = {"dock_launch_shape": st["dock_shape"], "grid_shape": st["grid_shape"]}
         dock_ms += st["dock_ms"]
@@ -567,7 +568,8 @@ def run_ours(a):
         "bfgs_evals_per_s": evals * world / elapsed,
         "bfgs_evals_per_step": evals / K,
         "plain": {"value": plain_value * world, "unit": UNIT, "batched_over_plain": value / (plain_value * world),
-                  **plain_split},
+                  "batched_over_plain_same_ligands": (B / step_wall[0]) / plain_value,
+                  "batched_same_ligands_value": B / step_wall[0], **plain_split},
         "batched_split": batched_split,
         "grid_build": {"ms": min(grid_ms), "points": n_pts, "types": 8,
                        "gbs": grid_bytes / (min(grid_ms) / 1e3) / 1e9,

@@ -28,9 +28,13 @@ struct PoseParams {
     int32_t warp_floats;
 };
 
-// mode 0: energy, 1: energy+gradient, 2: coordinates, 3: local optimisation
+// mode 0: energy, 1: energy+gradient, 2: coordinates, 3: local optimisation.
+// Modes 0-2 are held to 64 registers (8 blocks of 4 warps per SM):
+// they fit without spills, and the adjoint (mode 1) left free takes 72 and
+// loses a block per SM.
+constexpr int pose_min_blocks(int mode) { return mode == 3 ? 1 : 8; }
 template <int mode>
-__global__ void __launch_bounds__(32 * kPoseWarps) pose_kernel(PoseParams p) {
+__global__ void __launch_bounds__(32 * kPoseWarps, pose_min_blocks(mode)) pose_kernel(PoseParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* base = reinterpret_cast<float*>(smem4) + size_t(wid) * p.warp_floats;
