@@ -229,10 +229,13 @@ int dock_shape_for(Ctx& c, const vd_search_params& sp, uint64_t key) {
     return kTunedShapes[c.dock_tune.pick(key, kNumTuned)];
 }
 
-void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals) {
-    if (!b.tuned || evals == 0) return;
+void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, const unsigned long long* lig_evals) {
+    if (!b.tuned) return;
+    double work = 0;
+    for (size_t i = 0; i < b.eval_bytes.size(); ++i) work += double(lig_evals[i]) * b.eval_bytes[i];
+    if (!(work > 0)) return;
     for (int i = 0; i < kNumTuned; ++i)
-        if (kTunedShapes[i] == b.shape) c.dock_tune.report(b.tune_key, i, ms / double(evals));
+        if (kTunedShapes[i] == b.shape) c.dock_tune.report(b.tune_key, i, ms / work);
 }
 
 // Heuristics of main.cpp:354-391 (atoms = all ligand atoms): search depth
@@ -280,6 +283,7 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
         uid[i] = uint32_t(ligs[i]);
         search_defaults(L, sp, depth[i], steps[i]);
         prefix[i + 1] = prefix[i] + sp.n_chains;
+        out.eval_bytes.push_back(32.0 * L.h.n_atoms + 16.0 * L.h.n_pairs);
         max_wf = std::max(max_wf, lig_warp_floats(L) + 4 * pad4(7 + L.h.ntors) + kChainWords +
                                       (sp.dense_bfgs ? dense_floats(L.h.ntors) : 0));
         max_nt = std::max(max_nt, L.h.ntors);
@@ -424,7 +428,7 @@ vd_status vd_mc_chains(vd_ctx* h, int32_t lig, const vd_search_params* sp, float
     VD_CUDA(cudaEventElapsedTime(&ms, c.ev0, c.ev1));
     c.stats.dock_ms = ms;
     c.stats.bfgs_evals += int64_t(ev);
-    dock_tune_report(c, b, ms, ev);
+    dock_tune_report(c, b, ms, &ev);
     if (evals) *evals = int64_t(ev);
     return VD_OK;
 }

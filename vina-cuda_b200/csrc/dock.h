@@ -18,6 +18,7 @@ struct DockBuffers {
     size_t extra_bytes = 0;         // caller-requested scratch after the outputs
     char* d_extra = nullptr;
     uint64_t tune_key = 0;          // autotuner key of the launch
+    std::vector<double> eval_bytes; // per ligand: algorithmic bytes of one evaluation (tuner cost unit)
     int shape = 0;                  // launch shape used (0-based)
     bool tuned = false;             // shape came from the autotuner
     std::vector<unsigned char> h_params;  // packed parameter arrays (host)
@@ -37,8 +38,11 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
 vd_status enqueue_dock(Ctx& c, const DockBuffers& b, const void* params_src, cudaStream_t stream);
 vd_status launch_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_params& sp, bool persistent,
                       DockBuffers& out, cudaStream_t stream);
-// Feeds the kernel time per search evaluation of a finished launch to the autotuner.
-void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, uint64_t evals);
+// Feeds a finished launch's kernel time to the autotuner, per unit of work:
+// ms / sum over ligands of (evaluations x algorithmic bytes per evaluation),
+// so shapes tried on different ligands of one workload compare fairly.
+// lig_evals: evaluations per ligand of the launch, in batch order.
+void dock_tune_report(Ctx& c, const DockBuffers& b, double ms, const unsigned long long* lig_evals);
 // Reads and clears the docking kernel's device bounds-check word (checked
 // build only; VD_OK otherwise).
 vd_status dock_take_checks(const char* where);

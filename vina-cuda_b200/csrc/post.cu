@@ -935,7 +935,7 @@ vd_status dock_pipeline(Ctx& c, const std::vector<int>& ligs, const vd_search_pa
     c.stats.dock_ms = dock_ms;
     c.stats.post_ms = post_ms;
     c.stats.bfgs_evals += int64_t(h_cnt[0] + h_cnt[1]);
-    dock_tune_report(c, db, dock_ms, h_cnt[0]);
+    dock_tune_report(c, db, dock_ms, h_cnt + 2);
     for (int i = 0; i < n; ++i) out[i].bfgs_evals = int64_t(h_cnt[2 + i]);  // search evaluations
     return VD_OK;
 }
