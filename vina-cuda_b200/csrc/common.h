@@ -1,6 +1,7 @@
 // Internal declarations shared by the vdock host code and CUDA kernels.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -85,10 +86,14 @@ static_assert(sizeof(LigHeader) == 64, "header size");
 // (xs type | node << 8 | element << 16) stored in .w as int bits.
 // Rigid body record: origin relative to parent frame, torsion axis in the
 // parent frame, parent index, atom range and subtree end (pre-order).
+// Three 16-byte words, grouped by use so the evaluation reads each with one
+// 128-bit load: {origin, parent} per step of the ancestor walk, {axis,
+// first atom} for the local rotation and the torsion derivative, and the
+// ranges (sub_atom_end last) for the subtree sums.
 struct NodeRec {
     float rel_origin[3];
-    float axis[3];
     int32_t parent;
+    float axis[3];
     int32_t atom_begin;
     int32_t atom_end;
     int32_t subtree_end;  // nodes [k, subtree_end) form k's subtree
@@ -96,6 +101,9 @@ struct NodeRec {
     int32_t sub_atom_end;  // heavy atoms [atom_begin, sub_atom_end) belong to k's subtree
 };
 static_assert(sizeof(NodeRec) == 48, "node size");
+static_assert(offsetof(NodeRec, parent) == 12 && offsetof(NodeRec, atom_begin) == 28 &&
+                  offsetof(NodeRec, sub_atom_end) == 44,
+              "node words");
 
 struct HostLigand {
     LigHeader h;

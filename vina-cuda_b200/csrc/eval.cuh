@@ -158,16 +158,22 @@ __device__ __forceinline__ void qmat_rows(float4 q, float* nd) {
     nd[10] = aa - bb - cc + dd;
 }
 
-// Phases 1-3a: rigid-body frames and heavy-atom coordinates from the pose in m.x.
-__device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, int lane) {
+// Node words as 128-bit loads (NodeRec: {origin, parent}, {axis, first
+// atom}, {atom end, subtree end, depth, subtree atom end}).
+__device__ __forceinline__ float4 node_word(const NodeRec* nodes, int k, int w) {
+    return __ldg(reinterpret_cast<const float4*>(nodes + k) + w);
+}
+
+// Phases 1-2: rigid-body frames from the pose in m.x.
+__device__ __forceinline__ void frames(const LigView& L, const WarpMem& m, int lane) {
     // 1: local rotation of each body about its axis (angle_to_quaternion)
     for (int k = lane; k < L.nn; k += 32) {
         float4 aa = make_float4(1.f, 0.f, 0.f, 0.f);
         if (k > 0) {
             float s, c;
             __sincosf(0.5f * m.x[7 + k - 1], &s, &c);  // |angle| <= pi/2, abs error < 1e-6
-            const NodeRec& n = L.nodes[k];
-            aa = make_float4(c, s * __ldg(&n.axis[0]), s * __ldg(&n.axis[1]), s * __ldg(&n.axis[2]));
+            const float4 ax = node_word(L.nodes, k, 1);
+            aa = make_float4(c, s * ax.x, s * ax.y, s * ax.z);
         }
         *reinterpret_cast<float4*>(m.nd + kNodeF * k + kNdAA) = aa;
     }
@@ -180,17 +186,16 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
         float3 w = make_float3(0.f, 0.f, 0.f);
         if (k > 0) {
             P = *reinterpret_cast<const float4*>(m.nd + kNodeF * k + kNdAA);
-            const NodeRec& nk = L.nodes[k];
-            w = make_float3(__ldg(&nk.rel_origin[0]), __ldg(&nk.rel_origin[1]), __ldg(&nk.rel_origin[2]));
-            int j = VD_DCLAMP(__ldg(&nk.parent), 0, k - 1, kChkParent);
+            const float4 ok = node_word(L.nodes, k, 0);
+            w = make_float3(ok.x, ok.y, ok.z);
+            int j = VD_DCLAMP(__float_as_int(ok.w), 0, k - 1, kChkParent);
             while (j > 0) {
                 const float4 aj = *reinterpret_cast<const float4*>(m.nd + kNodeF * j + kNdAA);
-                const NodeRec& nj = L.nodes[j];
+                const float4 oj = node_word(L.nodes, j, 0);
                 const float3 r = qrot(aj, w);
-                w = make_float3(__ldg(&nj.rel_origin[0]) + r.x, __ldg(&nj.rel_origin[1]) + r.y,
-                                __ldg(&nj.rel_origin[2]) + r.z);
+                w = make_float3(oj.x + r.x, oj.y + r.y, oj.z + r.z);
                 P = qmul(aj, P);
-                j = VD_DCLAMP(__ldg(&nj.parent), 0, j - 1, kChkParent);
+                j = VD_DCLAMP(__float_as_int(oj.w), 0, j - 1, kChkParent);
             }
         }
         float4 q = qmul(qr, P);
@@ -203,16 +208,21 @@ __device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, i
         qmat_rows(q, nd);
     }
     __syncwarp();
-    // 3a: heavy-atom coordinates
-    for (int i = lane; i < L.na; i += 32) {
-        const float4 a = __ldg(&L.atoms[i]);
-        const int k = VD_DCLAMP((__float_as_int(a.w) >> 8) & 0xff, 0, L.nn - 1, kChkAtomBody);
-        const float4* nd = reinterpret_cast<const float4*>(m.nd + kNodeF * k);
-        const float4 r0 = nd[0], r1 = nd[1], r2 = nd[2];
-        m.c[i] = make_float4(r0.w + (r0.x * a.x + r0.y * a.y + r0.z * a.z),
-                             r1.w + (r1.x * a.x + r1.y * a.y + r1.z * a.z),
-                             r2.w + (r2.x * a.x + r2.y * a.y + r2.z * a.z), 0.f);
-    }
+}
+
+// Phase 3a for one heavy atom: its coordinates from its body's frame.
+__device__ __forceinline__ float4 atom_position(const LigView& L, const WarpMem& m, float4 a) {
+    const int k = VD_DCLAMP((__float_as_int(a.w) >> 8) & 0xff, 0, L.nn - 1, kChkAtomBody);
+    const float4* nd = reinterpret_cast<const float4*>(m.nd + kNodeF * k);
+    const float4 r0 = nd[0], r1 = nd[1], r2 = nd[2];
+    return make_float4(r0.w + (r0.x * a.x + r0.y * a.y + r0.z * a.z), r1.w + (r1.x * a.x + r1.y * a.y + r1.z * a.z),
+                       r2.w + (r2.x * a.x + r2.y * a.y + r2.z * a.z), 0.f);
+}
+
+// Phases 1-3a: rigid-body frames and heavy-atom coordinates from the pose in m.x.
+__device__ __forceinline__ void kinematics(const LigView& L, const WarpMem& m, int lane) {
+    frames(L, m, lane);
+    for (int i = lane; i < L.na; i += 32) m.c[i] = atom_position(L, m, __ldg(&L.atoms[i]));
     __syncwarp();
 }
 
@@ -313,13 +323,16 @@ struct GridInter {
 template <bool want_grad, bool pair_atomics = false, class Inter>
 __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const Inter& inter, const float4* smooth,
                              float v_intra, float fix, float inv_fix, int lane) {
-    kinematics(L, m, lane);
+    frames(L, m, lane);
     float e = 0.f;
-    // 3b: grid term per atom; its gradient seeds the atom's force
+    // 3: per atom its coordinates (kept for the pair phase) and the grid
+    // term, whose gradient seeds the atom's force
     for (int i = lane; i < L.na; i += 32) {
-        const int t = __float_as_int(__ldg(&L.atoms[i].w)) & 0xff;
+        const float4 a = __ldg(&L.atoms[i]);
+        const float4 ci = atom_position(L, m, a);
+        m.c[i] = ci;
+        const int t = __float_as_int(a.w) & 0xff;
         float gx, gy, gz;
-        const float4 ci = m.c[i];
         e += inter(t, ci.x, ci.y, ci.z, gx, gy, gz);
         if (want_grad) {
             int* const q = reinterpret_cast<int*>(m.ns);  // pair-force accumulators start at zero
@@ -328,7 +341,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             q[i] = 0; q[a4 + i] = 0; q[2 * a4 + i] = 0;
         }
     }
-    if (want_grad) __syncwarp();
+    __syncwarp();
     // 4: intra pairs, two per lane per iteration (two table gathers in
     // flight); table indices are clamped and pairs past the cutoff masked
     // (their table loads predicated off).
@@ -525,8 +538,9 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     __syncwarp();
     // 7: subtree sums (prefix differences), torques and the pose gradient
     for (int k = lane; k < L.nn; k += 32) {
-        const int e1 = VD_DCLAMP(__ldg(&L.nodes[k].sub_atom_end), 0, L.na, kChkSubtree);
-        const int b = VD_DCLAMP(__ldg(&L.nodes[k].atom_begin), 0, e1, kChkSubtree);
+        const float4 w1 = node_word(L.nodes, k, 1);  // {axis, first atom}
+        const int e1 = VD_DCLAMP(__float_as_int(node_word(L.nodes, k, 2).w), 0, L.na, kChkSubtree);
+        const int b = VD_DCLAMP(__float_as_int(w1.w), 0, e1, kChkSubtree);
         const int a4 = pad4(L.na);
         float F0 = 0.f, F1 = 0.f, F2 = 0.f, M0 = 0.f, M1 = 0.f, M2 = 0.f;
         if (e1 > b) {
@@ -547,8 +561,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const float T0 = M0 - (dy * F2 - dz * F1);
             const float T1 = M1 - (dz * F0 - dx * F2);
             const float T2 = M2 - (dx * F1 - dy * F0);
-            const NodeRec& n = L.nodes[k];
-            const float u0 = __ldg(&n.axis[0]), u1 = __ldg(&n.axis[1]), u2 = __ldg(&n.axis[2]);
+            const float u0 = w1.x, u1 = w1.y, u2 = w1.z;
             const float a0 = nd[0] * u0 + nd[1] * u1 + nd[2] * u2;
             const float a1 = nd[4] * u0 + nd[5] * u1 + nd[6] * u2;
             const float a2 = nd[8] * u0 + nd[9] * u1 + nd[10] * u2;
