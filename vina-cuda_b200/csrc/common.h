@@ -57,11 +57,13 @@ void set_error(const std::string& msg);
 // lane reads entry k*32 + l: one coalesced 512-byte warp load per two pairs.
 // A lane's odd last pair is repeated in the int4's second half.
 // The search schedule holds the same pairs again in rounds of up to 32, one
-// pair per lane per round, two rounds per int4 (entry k*32 + l: rounds 2k
-// and 2k+1 of lane l), arranged so that the lanes of a round touch as few
-// equal atoms as possible: the search adds both atoms' pair forces with
-// shared-memory atomics, and on B200 atomics of several lanes to one address
-// serialise.  An unused slot has type pair -1.
+// pair per lane per round, each pair one 32-bit word (a | b << 8 | type pair
+// << 16), two rounds per int2 (entry k*32 + l: rounds 2k and 2k+1 of lane
+// l, one coalesced 256-byte warp load), arranged so that the lanes of a
+// round touch as few equal atoms as possible: the search adds both atoms'
+// pair forces with shared-memory atomics, and on B200 atomics of several
+// lanes to one address serialise.  An unused slot is 0xffff0000 (atoms 0
+// and 0, negative as a signed word).
 // Only heavy atoms (XS type >= 0) are on the device; hydrogens carry no
 // energy and are placed on the host when output files are written.
 struct LigHeader {
@@ -75,8 +77,8 @@ struct LigHeader {
     int32_t max_depth;
     int32_t off_lpairs;   // lane-pair int4 entries start (16-byte word offset)
     int32_t lp_iters;     // int4 entries per lane (longest segment, two pairs each)
-    int32_t off_spairs;   // search-schedule int4 entries start (16-byte word offset)
-    int32_t sp_iters;     // int4 entries per lane of the search schedule (two rounds each)
+    int32_t off_spairs;   // search-schedule int2 entries start (16-byte word offset)
+    int32_t sp_iters;     // int2 entries per lane of the search schedule (two rounds each)
     float num_tors;       // N_tors of the conf-independent term
     float pad3, pad4, pad5;
 };

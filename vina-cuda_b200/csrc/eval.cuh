@@ -54,7 +54,7 @@ struct LigView {
     const NodeRec* nodes;
     const int2* pairs;
     const int4* lpairs;         // per-lane segments, two pairs per entry, interleaved by lane
-    const int4* spairs;         // search schedule: rounds of one pair per lane, two rounds per entry
+    const int2* spairs;         // search schedule: rounds of one pair per lane, two rounds per entry
     int32_t na, nn, np, nt;
     int32_t sp_iters;           // schedule entries per lane
     float num_tors;
@@ -73,16 +73,17 @@ __device__ __forceinline__ LigView lig_view(const float4* pool, int64_t off) {
     L.nodes = reinterpret_cast<const NodeRec*>(b + h->off_nodes);
     L.pairs = reinterpret_cast<const int2*>(b + h->off_pairs);
     L.lpairs = reinterpret_cast<const int4*>(b + h->off_lpairs);
-    L.spairs = reinterpret_cast<const int4*>(b + h->off_spairs);
+    L.spairs = reinterpret_cast<const int2*>(b + h->off_spairs);
     L.sp_iters = h->sp_iters;
     return L;
 }
 
 // Body frame in shared memory, 20 floats: three rows [R(i,0) R(i,1) R(i,2) o_i]
-// (so an atom position is three 128-bit loads), the quaternion and the
-// local rotation about the body's torsion axis.
+// (so an atom position is three 128-bit loads), 4 unused, and the local
+// rotation about the body's torsion axis.  The 80-byte stride puts the
+// 128-bit rows of 8 consecutive bodies in distinct bank groups.
 constexpr int kNodeF = 20;
-constexpr int kNdQ = 12, kNdAA = 16;
+constexpr int kNdAA = 16;
 
 __host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
 // Shared-memory floats one warp needs for a ligand of the given size.
@@ -141,21 +142,16 @@ __device__ __forceinline__ float3 qrot(float4 q, float3 v) {
     return make_float3(v.x + 2.f * (q.z * tz - q.w * ty), v.y + 2.f * (q.w * tx - q.y * tz),
                        v.z + 2.f * (q.y * ty - q.z * tx));
 }
-// Rotation matrix of a unit quaternion (quaternion.cpp:155-192), written as
-// the rows of the body frame: nd[4*i + j] = R(i, j).
-__device__ __forceinline__ void qmat_rows(float4 q, float* nd) {
+// Body frame from a unit quaternion (rotation matrix as quaternion.cpp:155-192)
+// and origin o, written as three 128-bit rows [R(i,0) R(i,1) R(i,2) o_i].
+__device__ __forceinline__ void store_frame(float4 q, float3 o, float* nd) {
     const float a = q.x, b = q.y, c = q.z, d = q.w;
     const float aa = a * a, ab = a * b, ac = a * c, ad = a * d, bb = b * b, bc = b * c, bd = b * d,
                 cc = c * c, cd = c * d, dd = d * d;
-    nd[0] = aa + bb - cc - dd;
-    nd[1] = 2.f * (-ad + bc);
-    nd[2] = 2.f * (ac + bd);
-    nd[4] = 2.f * (ad + bc);
-    nd[5] = aa - bb + cc - dd;
-    nd[6] = 2.f * (-ab + cd);
-    nd[8] = 2.f * (-ac + bd);
-    nd[9] = 2.f * (ab + cd);
-    nd[10] = aa - bb - cc + dd;
+    float4* r = reinterpret_cast<float4*>(nd);
+    r[0] = make_float4(aa + bb - cc - dd, 2.f * (-ad + bc), 2.f * (ac + bd), o.x);
+    r[1] = make_float4(2.f * (ad + bc), aa - bb + cc - dd, 2.f * (-ab + cd), o.y);
+    r[2] = make_float4(2.f * (-ac + bd), 2.f * (ab + cd), aa - bb - cc + dd, o.z);
 }
 
 // Node words as 128-bit loads (NodeRec: {origin, parent}, {axis, first
@@ -179,8 +175,11 @@ __device__ __forceinline__ void frames(const LigView& L, const WarpMem& m, int l
     }
     __syncwarp();
     // 2: frames by walking the ancestor path
-    const float4 qr = make_float4(m.x[3], m.x[4], m.x[5], m.x[6]);
-    const float3 orr = make_float3(m.x[0], m.x[1], m.x[2]);
+    // the pose's position and orientation: two broadcast 128-bit loads (m.x is
+    // 16-byte aligned and holds at least 8 floats)
+    const float4 x0 = *reinterpret_cast<const float4*>(m.x), x1 = *reinterpret_cast<const float4*>(m.x + 4);
+    const float4 qr = make_float4(x0.w, x1.x, x1.y, x1.z);
+    const float3 orr = make_float3(x0.x, x0.y, x0.z);
     for (int k = lane; k < L.nn; k += 32) {
         float4 P = make_float4(1.f, 0.f, 0.f, 0.f);
         float3 w = make_float3(0.f, 0.f, 0.f);
@@ -202,10 +201,7 @@ __device__ __forceinline__ void frames(const LigView& L, const WarpMem& m, int l
         const float inv = rsqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
         q = make_float4(q.x * inv, q.y * inv, q.z * inv, q.w * inv);
         const float3 ro = qrot(qr, w);
-        float* nd = m.nd + kNodeF * k;
-        *reinterpret_cast<float4*>(nd + kNdQ) = q;
-        nd[3] = orr.x + ro.x; nd[7] = orr.y + ro.y; nd[11] = orr.z + ro.z;
-        qmat_rows(q, nd);
+        store_frame(q, make_float3(orr.x + ro.x, orr.y + ro.y, orr.z + ro.z), m.nd + kNodeF * k);
     }
     __syncwarp();
 }
@@ -355,14 +351,14 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         int* const qx = reinterpret_cast<int*>(m.ns);
         int* const qy = qx + pad4(L.na);
         int* const qz = qy + pad4(L.na);
-        const int4* sp = L.spairs + lane;
+        const int2* sp = L.spairs + lane;
         for (int k = 0; k < L.sp_iters; ++k, sp += 32) {
-            const int4 qq = __ldg(sp);  // coalesced across the warp
-            const bool v0 = qq.y >= 0, v1 = qq.w >= 0;  // unused slots carry type pair -1
-            const int a0 = VD_DCLAMP(qq.x & 0xffff, 0, L.na - 1, kChkPairAtom);
-            const int b0 = VD_DCLAMP(qq.x >> 16, 0, L.na - 1, kChkPairAtom);
-            const int a1 = VD_DCLAMP(qq.z & 0xffff, 0, L.na - 1, kChkPairAtom);
-            const int b1 = VD_DCLAMP(qq.z >> 16, 0, L.na - 1, kChkPairAtom);
+            const int2 qq = __ldg(sp);  // coalesced across the warp
+            const bool v0 = qq.x >= 0, v1 = qq.y >= 0;  // unused slots are negative (atoms 0, 0)
+            const int a0 = VD_DCLAMP(qq.x & 0xff, 0, L.na - 1, kChkPairAtom);
+            const int b0 = VD_DCLAMP((qq.x >> 8) & 0xff, 0, L.na - 1, kChkPairAtom);
+            const int a1 = VD_DCLAMP(qq.y & 0xff, 0, L.na - 1, kChkPairAtom);
+            const int b1 = VD_DCLAMP((qq.y >> 8) & 0xff, 0, L.na - 1, kChkPairAtom);
             const float4 ca0 = m.c[a0], cb0 = m.c[b0], ca1 = m.c[a1], cb1 = m.c[b1];
             const float r0x = cb0.x - ca0.x, r0y = cb0.y - ca0.y, r0z = cb0.z - ca0.z;
             const float r1x = cb1.x - ca1.x, r1y = cb1.y - ca1.y, r1z = cb1.z - ca1.z;
@@ -370,8 +366,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             const float rf0 = fminf(32.f * d0, 2047.5f), rf1 = fminf(32.f * d1, 2047.5f);
             const int i0 = VD_DCLAMP(int(rf0), 0, kBins - 2, kChkTableBin);
             const int i1 = VD_DCLAMP(int(rf1), 0, kBins - 2, kChkTableBin);
-            const int tp0 = VD_DCLAMP(v0 ? qq.y : 0, 0, kPairTypes - 1, kChkPairType);
-            const int tp1 = VD_DCLAMP(v1 ? qq.w : 0, 0, kPairTypes - 1, kChkPairType);
+            const int tp0 = VD_DCLAMP(v0 ? (qq.x >> 16) : 0, 0, kPairTypes - 1, kChkPairType);
+            const int tp1 = VD_DCLAMP(v1 ? (qq.y >> 16) : 0, 0, kPairTypes - 1, kChkPairType);
             const bool in0 = v0 && d0 < 64.f, in1 = v1 && d1 < 64.f;
             float4 t0 = make_float4(0.f, 0.f, 0.f, 0.f), t1 = t0;
             if (in0) t0 = __ldg(smooth + size_t(tp0) * kBins + i0);  // no gather past the cutoff
@@ -487,7 +483,8 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     // origin.  Atoms are grouped by body in pre-order, so a subtree's atoms
     // are one contiguous range and its sums are a difference of two prefixes.
     // Lane l owns atoms [l*A, l*A + A); prefix forces overwrite fx/fy/fz.
-    const float ox = m.x[0], oy = m.x[1], oz = m.x[2];
+    const float4 xo4 = *reinterpret_cast<const float4*>(m.x);
+    const float ox = xo4.x, oy = xo4.y, oz = xo4.z;
     {
         const int A = (L.na + 31) >> 5, a0 = lane * A, a1 = min(L.na, a0 + A);
         const int a4 = pad4(L.na);
@@ -556,15 +553,16 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         if (k == 0) {
             m.g[0] = F0; m.g[1] = F1; m.g[2] = F2; m.g[3] = M0; m.g[4] = M1; m.g[5] = M2;
         } else {
-            const float* nd = m.nd + kNodeF * k;
-            const float dx = nd[3] - ox, dy = nd[7] - oy, dz = nd[11] - oz;
+            const float4* nd = reinterpret_cast<const float4*>(m.nd + kNodeF * k);
+            const float4 r0 = nd[0], r1 = nd[1], r2 = nd[2];
+            const float dx = r0.w - ox, dy = r1.w - oy, dz = r2.w - oz;
             const float T0 = M0 - (dy * F2 - dz * F1);
             const float T1 = M1 - (dz * F0 - dx * F2);
             const float T2 = M2 - (dx * F1 - dy * F0);
             const float u0 = w1.x, u1 = w1.y, u2 = w1.z;
-            const float a0 = nd[0] * u0 + nd[1] * u1 + nd[2] * u2;
-            const float a1 = nd[4] * u0 + nd[5] * u1 + nd[6] * u2;
-            const float a2 = nd[8] * u0 + nd[9] * u1 + nd[10] * u2;
+            const float a0 = r0.x * u0 + r0.y * u1 + r0.z * u2;
+            const float a1 = r1.x * u0 + r1.y * u1 + r1.z * u2;
+            const float a2 = r2.x * u0 + r2.y * u1 + r2.z * u2;
             m.g[6 + k - 1] = T0 * a0 + T1 * a1 + T2 * a2;
         }
     }

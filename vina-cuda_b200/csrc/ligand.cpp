@@ -294,14 +294,23 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     H.off_spairs = H.off_lpairs + std::max<int32_t>(1, int32_t(lpairs.size()));
     const std::vector<std::vector<int2>> rounds = schedule_pairs(pairs, nh);
     H.sp_iters = int32_t((rounds.size() + 1) / 2);
-    std::vector<int4> spairs(size_t(32) * H.sp_iters, make_int4(0, -1, 0, -1));
+    static_assert(kMaxHeavy <= 256 && kPairTypes < 32768, "schedule word fields");
+    // one 32-bit word per scheduled pair: a | b << 8 | type pair << 16
+    // (heavy atoms < 128, type pairs < 153).  An unused slot has atoms 0 and
+    // 0 and type field 0xffff (a negative word): the kernel loads both atoms'
+    // coordinates before it tests the slot, so its atom fields must index
+    // real atoms.
+    constexpr int kUnusedSlot = -65536;  // 0xffff0000
+    std::vector<int2> spairs(size_t(32) * H.sp_iters, make_int2(kUnusedSlot, kUnusedSlot));
     for (size_t r = 0; r < rounds.size(); ++r)
         for (size_t l = 0; l < rounds[r].size(); ++l) {
-            int4& e = spairs[(r / 2) * 32 + l];
-            if (r % 2 == 0) { e.x = rounds[r][l].x; e.y = rounds[r][l].y; }
-            else { e.z = rounds[r][l].x; e.w = rounds[r][l].y; }
+            const int2 q = rounds[r][l];
+            const int w = (q.x & 0xff) | (((q.x >> 16) & 0xff) << 8) | (q.y << 16);
+            int2& e = spairs[(r / 2) * 32 + l];
+            if (r % 2 == 0) e.x = w;
+            else e.y = w;
         }
-    const int32_t total = H.off_spairs + std::max<int32_t>(1, int32_t(spairs.size()));
+    const int32_t total = H.off_spairs + std::max<int32_t>(1, words(spairs.size() * sizeof(int2)));
     H.num_tors = float(d->num_tors);
     L.blob.assign(size_t(total), make_float4(0, 0, 0, 0));
     char* base = reinterpret_cast<char*>(L.blob.data());
@@ -310,7 +319,7 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     std::memcpy(base + 16 * size_t(H.off_nodes), nodes.data(), nodes.size() * sizeof(NodeRec));
     if (P) std::memcpy(base + 16 * size_t(H.off_pairs), pairs.data(), pairs.size() * sizeof(int2));
     if (!lpairs.empty()) std::memcpy(base + 16 * size_t(H.off_lpairs), lpairs.data(), lpairs.size() * sizeof(int4));
-    if (!spairs.empty()) std::memcpy(base + 16 * size_t(H.off_spairs), spairs.data(), spairs.size() * sizeof(int4));
+    if (!spairs.empty()) std::memcpy(base + 16 * size_t(H.off_spairs), spairs.data(), spairs.size() * sizeof(int2));
     L.heavy_index = heavy_index;
     L.n_all_atoms = na;
     L.num_tors = d->num_tors;

@@ -714,7 +714,7 @@ vd_status prepare_post(Ctx& c, const std::vector<int>& ligs, const vd_search_par
         max_na = std::max(max_na, L.h.n_atoms);
         max_nn = std::max(max_nn, L.h.n_nodes);
     }
-    int sort_n = 1;
+    int sort_n = 2;  // >= 2: the warp's arrays after the 8-byte keys start 16-byte aligned
     while (sort_n < max_chains) sort_n <<= 1;
     VD_CHECK(sort_n <= 16384, VD_ERR_CAPACITY, "more than 16384 chains per ligand");
     std::vector<int32_t> plig(size_t(n) * VD_MAX_MODES), nin(n, VD_MAX_MODES);
