@@ -197,6 +197,24 @@ inline cudaError_t record_event(cudaEvent_t e, cudaStream_t s) {
                                                : cudaEventRecord(e, s);
 }
 
+// Each SM's on-chip data memory is split between shared memory and L1.  Asks
+// for the smallest shared-memory carve-out that holds `blocks` resident
+// blocks of `smem` bytes each (plus the driver's per-block reservation); the
+// percentage is rounded up and the driver rounds it up again to a capacity
+// it supports.  The rest is L1, which caches the kernels' table and grid
+// gathers.
+template <class K>
+inline cudaError_t prefer_l1(K kernel, int device, int blocks, size_t smem) {
+    int max_sm = 0, reserved = 0;
+    cudaError_t r = cudaDeviceGetAttribute(&max_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device);
+    if (r == cudaSuccess) r = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device);
+    if (r != cudaSuccess || max_sm <= 0) return r;
+    const size_t need = size_t(blocks) * (smem + size_t(reserved));
+    size_t pct = (need * 100 + size_t(max_sm) - 1) / size_t(max_sm);
+    if (pct > 100) pct = 100;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(pct));
+}
+
 vd_status ensure_scratch(Ctx* c, size_t bytes);
 // Context-owned device allocation: VD_ERR_NOMEM past the context's cap or
 // when the device is out of memory; *p is null on failure.

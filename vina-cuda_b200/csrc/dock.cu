@@ -186,6 +186,9 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
     if (lane == 0 && evals) atomicAdd(p.evals, (unsigned long long)evals);
 }
 
+// Resident 4-warp blocks per SM each launch shape's register budget targets.
+constexpr int kShapeBlocks[] = {8, 10, 12, 6, 4};
+
 using DockFn = void (*)(DockParams);
 template <bool persistent>
 DockFn dock_fn(int shape) {
@@ -359,6 +362,7 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     const DockFn k = sp.dense_bfgs ? (persistent ? dense_dock_fn<true>(out.shape) : dense_dock_fn<false>(out.shape))
                                    : (persistent ? dock_fn<true>(out.shape) : dock_fn<false>(out.shape));
     VD_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    VD_CUDA(prefer_l1(k, c.device, kShapeBlocks[out.shape], smem));
     int blocks = (items + wpb - 1) / wpb;
     if (persistent) {
         int per_sm = 0;

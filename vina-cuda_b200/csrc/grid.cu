@@ -431,6 +431,17 @@ vd_status vd_build_grids(vd_ctx* h, const int32_t* types, int32_t n_types) {
     if (c.grid_shape_fixed > 0) shapes.push_back(c.grid_shape_fixed - 1);
     else if (c.grid_tune.best(key) >= 0) shapes.push_back(c.grid_tune.best(key));
     else shapes = {0, 1};
+    // shared-memory carve-out for the blocks each tile keeps resident (2 of
+    // 256 threads or 4 of 128), the rest of the SM's data memory as L1
+    auto carve = [&](auto kern, int blocks) -> cudaError_t {
+        cudaFuncAttributes fa{};
+        const cudaError_t r = cudaFuncGetAttributes(&fa, kern);
+        return r != cudaSuccess ? r : prefer_l1(kern, c.device, blocks, fa.sharedSizeBytes);
+    };
+    VD_CUDA(carve(grid_build_kernel<4, 8>, 2));
+    VD_CUDA(carve(grid_build_kernel<8, 8>, 2));
+    VD_CUDA(carve(grid_build_kernel<4, 4>, 4));
+    VD_CUDA(carve(grid_build_kernel<8, 4>, 4));
     float best_ms = -1;
     for (int shape : shapes) {
         const int tz = shape == 0 ? 8 : 4;

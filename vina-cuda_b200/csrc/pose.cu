@@ -110,6 +110,7 @@ vd_status run_pose_kernel(Ctx& c, int lig, int n_poses, const float* d_poses, co
     VD_CHECK(smem <= 227 * 1024, VD_ERR_CAPACITY, "ligand too large for the pose kernel");
     auto kern = pose_kernel<mode>;
     VD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    if (mode != 3) VD_CUDA(prefer_l1(kern, c.device, pose_min_blocks(mode), smem));
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c.device);
     const int blocks = std::min((n_poses + kPoseWarps - 1) / kPoseWarps, dev_sms * 16);
