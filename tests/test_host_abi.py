@@ -224,6 +224,25 @@ def test_pair_force_scale_host_check(tmp_path):
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
 
 
+def test_pair_schedule_host_check(tmp_path):
+    """The docking search's pair schedule (csrc/schedule.cpp) on 200 random
+    pair sets of 10-128 atoms: every pair scheduled once with its type pair,
+    32-lane rounds, deterministic, and a layout search that never raises a
+    round's conflict cost (a compiled host check)."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("no host C++ compiler")
+    exe = tmp_path / "schedule_check"
+    inc = os.path.join(REPO, "vina-cuda_b200", "csrc")
+    srcs = [os.path.join(REPO, "tests", "host", "schedule_check.cpp"), os.path.join(inc, "schedule.cpp")]
+    subprocess.run([gxx, "-std=c++17", "-O2", "-Wall", "-I", inc, "-I", "/usr/local/cuda/include", *srcs, "-o",
+                    str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.startswith("OK"), r.stdout + r.stderr
+
+
 def _mutate(lines, rng):
     keys = ["ROOT", "ENDROOT", "BRANCH   1   2", "ENDBRANCH   1   2", "TORSDOF 3", "MODEL 1", "ENDMDL", "BRANCH",
             "BRANCH 9999 1", "ENDBRANCH 5 5", ""]

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "common.h"
+#include "schedule.h"
 
 namespace vd {
 
@@ -82,73 +83,6 @@ std::vector<int2> order_pairs(const std::vector<int2>& in) {
         r0 = r1;
     }
     return out;
-}
-
-// The search's pair schedule: rounds of up to 32 pairs (one per lane) in
-// which as few lanes as possible share an atom, so that the six atomic adds
-// of a round (force on each atom of the pair, x, y, z) rarely serialise.
-// Greedy per round over the remaining pairs, those whose atoms have the most
-// pairs left first: take pairs whose first atom and second atom are each
-// still unused in the round (either orientation: a pair's force is antisymmetric),
-// then allow two lanes per atom, then three, and so on, until the round holds
-// 32 pairs.  Within a round, lanes are then assigned so that each group of 8
-// lanes (one phase of a 128-bit shared-memory load of the atoms'
-// coordinates) sees distinct atom-index residues mod 8 where possible.
-// Returns the rounds as pairs {a | b << 16, type pair}.
-std::vector<std::vector<int2>> schedule_pairs(const std::vector<int2>& pairs, int na) {
-    std::vector<int> deg(na, 0);
-    for (const int2& q : pairs) { ++deg[q.x & 0xffff]; ++deg[q.x >> 16]; }
-    std::vector<int2> rem(pairs);
-    std::vector<std::vector<int2>> rounds;
-    std::vector<int> ca(na), cb(na);
-    while (!rem.empty()) {
-        std::stable_sort(rem.begin(), rem.end(), [&](const int2& x, const int2& y) {
-            return deg[x.x & 0xffff] + deg[x.x >> 16] > deg[y.x & 0xffff] + deg[y.x >> 16];
-        });
-        std::fill(ca.begin(), ca.end(), 0);
-        std::fill(cb.begin(), cb.end(), 0);
-        std::vector<int2> take;
-        for (int cap = 1; take.size() < 32 && !rem.empty(); ++cap) {
-            std::vector<int2> keep;
-            for (const int2& q : rem) {
-                const int u = q.x & 0xffff, v = q.x >> 16;
-                if (take.size() < 32 && ca[u] < cap && cb[v] < cap) {
-                    take.push_back(q);
-                    ++ca[u]; ++cb[v];
-                } else if (take.size() < 32 && ca[v] < cap && cb[u] < cap) {
-                    take.push_back(make_int2(v | (u << 16), q.y));
-                    ++ca[v]; ++cb[u];
-                } else {
-                    keep.push_back(q);
-                }
-            }
-            rem.swap(keep);
-        }
-        for (const int2& q : take) { --deg[q.x & 0xffff]; --deg[q.x >> 16]; }
-        // lanes: phases of 8 with distinct residues mod 8 of both atoms, then of one, then any
-        std::vector<int2> left(take), order;
-        while (!left.empty()) {
-            std::vector<int2> phase;
-            unsigned ga = 0, gb = 0;
-            for (int strict = 2; strict >= 0; --strict) {
-                std::vector<int2> keep;
-                for (const int2& q : left) {
-                    const unsigned ra = 1u << ((q.x & 0xffff) & 7), rb = 1u << ((q.x >> 16) & 7);
-                    const bool oka = !(ga & ra), okb = !(gb & rb);
-                    if (phase.size() < 8 && (strict == 0 || (strict == 1 && (oka || okb)) || (oka && okb))) {
-                        phase.push_back(q);
-                        ga |= ra; gb |= rb;
-                    } else {
-                        keep.push_back(q);
-                    }
-                }
-                left.swap(keep);
-            }
-            order.insert(order.end(), phase.begin(), phase.end());
-        }
-        rounds.push_back(order);
-    }
-    return rounds;
 }
 
 }  // namespace
@@ -305,6 +239,7 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     for (size_t r = 0; r < rounds.size(); ++r)
         for (size_t l = 0; l < rounds[r].size(); ++l) {
             const int2 q = rounds[r][l];
+            if (q.y < 0) continue;  // empty lane
             const int w = (q.x & 0xff) | (((q.x >> 16) & 0xff) << 8) | (q.y << 16);
             int2& e = spairs[(r / 2) * 32 + l];
             if (r % 2 == 0) e.x = w;
