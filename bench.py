@@ -126,17 +126,17 @@ def lig_bytes(lig):
 # DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
 # captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
 # ligands x 6,500 chains, 11.55 M evaluations per launch): 80 registers
-# 5.60 GB per launch.  The bench scales the figure by the evaluations of
+# 5.58 GB per launch.  The bench scales the figure by the evaluations of
 # each launch; shapes not captured report no traffic.
-DOCK_DRAM_BYTES_PER_EVAL = {4: 485.0}
+DOCK_DRAM_BYTES_PER_EVAL = {4: 482.7}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 # L1 data-pipe (LSU) wavefronts of one grid build of this workload (188^3
 # points x 8 maps, 8,000-atom receptor), from the ncu capture summarised in
 # profiles/grid_build_kernel_70A_8types.txt (l1tex__data_pipe_lsu_wavefronts.sum
 # of one grid_build_kernel launch).  The kernel's limit is that pipe: one
 # wavefront per SM per cycle; every in-range (point, receptor atom) pair reads
-# one 32-byte table row, one wavefront.
-GRID_L1_WAVEFRONTS = 133_836_283
+# one 32-byte table row, about one wavefront.
+GRID_L1_WAVEFRONTS = 128_461_116
 
 
 def grid_l1_roof(ms, clk, device):
