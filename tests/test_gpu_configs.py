@@ -29,7 +29,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as O
-from conftest import has_gpu
+from conftest import has_gpu, outside_box_energy_slack
 
 pytestmark = pytest.mark.gpu
 
@@ -160,7 +160,6 @@ def test_adjoint_all_65536_poses(vd):
     x = ctx.pose_coords(lc, poses)
     grid = orc.grid_info()
     npts, b, e = grid
-    cell = (e - b) / (npts - 1)
     inside = np.all((x >= b + 1e-3) & (x <= e - 1e-3), axis=(1, 2))
     assert inside.sum() >= n // 2, inside.sum()
     pairs = np.asarray(lig["pairs"]).reshape(-1, 2)
@@ -177,11 +176,7 @@ def test_adjoint_all_65536_poses(vd):
             worst_low = max(worst_low, de)
         if not inside[i]:
             xr = orc.coords(lo, c, lig["n_atoms"])[heavy]
-            out = (xr < b) | (xr > e) | (x[i] < b) | (x[i] > e)  # [atom][axis]
-            s_cells = np.abs((x[i].astype(np.float64) - b) / cell)
-            ulps = (np.spacing(s_cells.astype(np.float32)).astype(np.float64) * cell +
-                    np.spacing(np.abs(x[i])).astype(np.float64))
-            tol = E_TOL + 1e-5 * abs(er) + 1e6 * float((np.abs(x[i] - xr) + 4 * ulps)[out].sum())
+            tol = E_TOL + 1e-5 * abs(er) + outside_box_energy_slack(x[i], xr, grid)
         assert de <= tol, (i, e_gpu[i], er, tol)
         gscale = max(1.0, np.abs(gr).max())
         dg = np.abs(g_gpu[i] - gr).max() / gscale
@@ -269,7 +264,18 @@ def test_batched_uneven_512_ligands_vs_oracle_pipeline(vd):
 def test_wide_box_screen_vs_oracle_pipeline(vd):
     """Eight ligands of the wide-box screen in one batched call (6,500 chains
     each, heuristic depth, refinement and rescoring) against the oracle's
-    pipeline with the same seeds."""
+    pipeline with the same seeds.
+
+    A ligand's best score is a best-of-6,500 search result, and FP32 and
+    FP64 chains on the same seeds part ways after a few line searches, so
+    the GPU and oracle scores of a ligand are two draws from that ligand's
+    best-of-6,500 distribution.  Its spread is measured on the GPU itself
+    (the same batch with 8 other seeds): every paired difference must lie
+    within 5 standard deviations of the difference of two draws, sqrt(2)
+    times the ligand's seed-to-seed standard deviation (at least 0.02
+    kcal/mol: ligands whose searches all reach the same minimum differ only
+    by the FP32/FP64 rounding of its refinement), and the median difference
+    within 0.15 kcal/mol (no systematic shift)."""
     from vdock import synth
     cfg = synth.CONFIGS["screen"]
     xyz, xs = synth.receptor(cfg["rec_atoms"], cfg["rec_radius"], SEED)
@@ -286,11 +292,16 @@ def test_wide_box_screen_vs_oracle_pipeline(vd):
     print(f"wide box: score diff median {np.median(d):.3f} |d| max {np.abs(d).max():.3f}; "
           f"top-pose RMSD {np.round(rows[:, 2], 2).tolist()}")
     print(np.round(rows, 3).tolist())
-    # 6,500 chains per ligand converge the best score: paired differences
-    # small in median and bounded for every ligand.  The top poses themselves
-    # may sit in different, near-degenerate sites of a 70 A box (equal scores
-    # tens of A apart), so their RMSD is reported, not bounded.
-    assert abs(np.median(d)) <= 0.15 and np.abs(d).max() <= 0.5, rows
+    # The top poses may sit in different, near-degenerate sites of a 70 A box
+    # (equal scores tens of A apart), so their RMSD is reported, not bounded.
+    seeds = np.array([[float(r["energy"][0]) for r in ctx.dock_batched(
+        ids, vd.search_params(seed=SEED + k, n_chains=cfg["chains"], search_depth=0, refine=1))]
+        for k in range(1, 9)])
+    sd = np.maximum(seeds.std(axis=0, ddof=1), 0.02)
+    z = d / (np.sqrt(2.0) * sd)
+    print(f"wide box: seed-to-seed sd {np.round(sd, 3).tolist()}, z {np.round(z, 2).tolist()}")
+    assert abs(np.median(d)) <= 0.15, rows
+    assert np.abs(z).max() <= 5.0, (rows, sd, z)
 
 
 def test_reference_docked_outputs_rescored_on_gpu(vd):

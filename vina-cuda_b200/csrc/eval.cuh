@@ -502,34 +502,47 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
             v[4] = dz * fx - dx * fz;
             v[5] = dx * fy - dy * fx;
         };
-        float run[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        for (int i = a0; i < a1; ++i) {
-            float v[6];
-            contrib(i, v);
+        auto scan = [&](float (&run)[6]) {  // inclusive scan of the lane totals
 #pragma unroll
-            for (int j = 0; j < 6; ++j) run[j] += v[j];
-        }
+            for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {  // inclusive scan of the lane totals
-#pragma unroll
-            for (int j = 0; j < 6; ++j) {
-                const float o = __shfl_up_sync(0xffffffffu, run[j], off);
-                if (lane >= off) run[j] += o;
+                for (int j = 0; j < 6; ++j) {
+                    const float o = __shfl_up_sync(0xffffffffu, run[j], off);
+                    if (lane >= off) run[j] += o;
+                }
             }
-        }
-        float acc[6];
+        };
+        if (A == 1) {  // up to 32 atoms: a lane's inclusive scan value is its atom's prefix
+            float run[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (a0 < a1) contrib(a0, run);
+            scan(run);
+            if (a0 < a1) {
+                m.fx[a0] = run[0]; m.fy[a0] = run[1]; m.fz[a0] = run[2];
+                mx[a0] = run[3]; my[a0] = run[4]; mz[a0] = run[5];
+            }
+        } else {  // lane totals, their exclusive scan, then each atom's prefix
+            float run[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            for (int i = a0; i < a1; ++i) {
+                float v[6];
+                contrib(i, v);
 #pragma unroll
-        for (int j = 0; j < 6; ++j) acc[j] = __shfl_up_sync(0xffffffffu, run[j], 1);
-        if (lane == 0)
+                for (int j = 0; j < 6; ++j) run[j] += v[j];
+            }
+            scan(run);
+            float acc[6];
 #pragma unroll
-            for (int j = 0; j < 6; ++j) acc[j] = 0.f;
-        for (int i = a0; i < a1; ++i) {
-            float v[6];
-            contrib(i, v);
+            for (int j = 0; j < 6; ++j) acc[j] = __shfl_up_sync(0xffffffffu, run[j], 1);
+            if (lane == 0)
 #pragma unroll
-            for (int j = 0; j < 6; ++j) acc[j] += v[j];
-            m.fx[i] = acc[0]; m.fy[i] = acc[1]; m.fz[i] = acc[2];
-            mx[i] = acc[3]; my[i] = acc[4]; mz[i] = acc[5];
+                for (int j = 0; j < 6; ++j) acc[j] = 0.f;
+            for (int i = a0; i < a1; ++i) {
+                float v[6];
+                contrib(i, v);
+#pragma unroll
+                for (int j = 0; j < 6; ++j) acc[j] += v[j];
+                m.fx[i] = acc[0]; m.fy[i] = acc[1]; m.fz[i] = acc[2];
+                mx[i] = acc[3]; my[i] = acc[4]; mz[i] = acc[5];
+            }
         }
     }
     __syncwarp();

@@ -75,6 +75,32 @@ __device__ __forceinline__ void warp_sum_n(float (&v)[N]) {
 #pragma unroll
         for (int j = 0; j < N; ++j) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
 }
+// Six sums over the warp, every lane getting all six: a reduce-scatter
+// (lanes exchange half of their partial sums with the lane 16, 8, then 4
+// away, so each lane ends with one of the sums over 8 lanes), a butterfly
+// over the remaining 4 lanes, then one broadcast per sum: 15 shuffles
+// instead of the 30 of six butterflies.
+__device__ __forceinline__ void warp_sum6(float (&v)[6], int lane) {
+    const unsigned full = 0xffffffffu;
+    const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+    const float w[8] = {v[0], v[1], v[2], v[3], v[4], v[5], 0.f, 0.f};
+    float a[4], b[2];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {  // sums 4*h16 + j
+        const float keep = h16 ? w[j + 4] : w[j], give = h16 ? w[j] : w[j + 4];
+        a[j] = keep + __shfl_xor_sync(full, give, 16);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {  // sums 4*h16 + 2*h8 + j
+        const float keep = h8 ? a[j + 2] : a[j], give = h8 ? a[j] : a[j + 2];
+        b[j] = keep + __shfl_xor_sync(full, give, 8);
+    }
+    float c = (h4 ? b[1] : b[0]) + __shfl_xor_sync(full, h4 ? b[0] : b[1], 4);  // sum 4*h16 + 2*h8 + h4
+    c += __shfl_xor_sync(full, c, 2);
+    c += __shfl_xor_sync(full, c, 1);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) v[j] = __shfl_sync(full, c, (j & 7) << 2);
+}
 __device__ __forceinline__ Vec2 vload(const float* g, int n, int lane) {
     Vec2 v;
     v.a = (lane < n) ? g[lane] : 0.f;
@@ -82,16 +108,14 @@ __device__ __forceinline__ Vec2 vload(const float* g, int n, int lane) {
     return v;
 }
 
-// x = xp + alpha * d (conf.h:367-372); xp, x in shared memory.
+// x = xp + alpha * d (conf.h:367-372); xp, x in shared memory.  Lanes 0-2
+// step the position components they hold; lane 3 rotates the orientation
+// by the rotation vector in lanes 3-5.
 __device__ __forceinline__ void conf_step(const float* xp, float* x, Vec2 d, float alpha, int nt, int lane) {
-    const float d0 = __shfl_sync(0xffffffffu, d.a, 0), d1 = __shfl_sync(0xffffffffu, d.a, 1),
-                d2 = __shfl_sync(0xffffffffu, d.a, 2), d3 = __shfl_sync(0xffffffffu, d.a, 3),
-                d4 = __shfl_sync(0xffffffffu, d.a, 4), d5 = __shfl_sync(0xffffffffu, d.a, 5);
-    if (lane == 0) {
-        x[0] = xp[0] + alpha * d0;
-        x[1] = xp[1] + alpha * d1;
-        x[2] = xp[2] + alpha * d2;
-        const float4 q = quat_increment(make_float4(xp[3], xp[4], xp[5], xp[6]), alpha * d3, alpha * d4, alpha * d5);
+    const float d4 = __shfl_down_sync(0xffffffffu, d.a, 1), d5 = __shfl_down_sync(0xffffffffu, d.a, 2);
+    if (lane < 3) x[lane] = xp[lane] + alpha * d.a;
+    if (lane == 3) {
+        const float4 q = quat_increment(make_float4(xp[3], xp[4], xp[5], xp[6]), alpha * d.a, alpha * d4, alpha * d5);
         x[3] = q.x; x[4] = q.y; x[5] = q.z; x[6] = q.w;
     }
     const int t0 = lane - 6, t1 = lane + 26;  // torsion held in slot a / b
@@ -174,7 +198,7 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
             const Vec2 dn = {-g.a, -g.b};
             float dots[6] = {lane_dot(g, g), lane_dot(yv, sv), lane_dot(yv, yv), lane_dot(sv, sv), lane_dot(gp, gp),
                              lane_dot(sv, dn)};
-            warp_sum_n(dots);
+            warp_sum6(dots, lane);
             if (!(sqrtf(dots[0]) >= 1e-5f)) return fx;
             if (max_steps <= k) break;
             ++k;
