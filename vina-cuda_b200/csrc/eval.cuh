@@ -238,7 +238,9 @@ __device__ __forceinline__ Corners load_corners(const MapView& G, const float* m
     if (cell) {
         const float* c = cell + ((size_t(a2) * (G.n[1] - 1) + a1) * (G.n[0] - 1) + a0) * 8;
         unsigned long long w0, w1, w2, w3;
-        asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];" : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3) : "l"(c));
+        // not allocated in L1: the cells of a 70 A box span 1.67 GB and are
+        // rarely re-read from L1, where they would evict the pair table
+        asm("ld.global.nc.L1::no_allocate.v4.b64 {%0,%1,%2,%3}, [%4];" : "=l"(w0), "=l"(w1), "=l"(w2), "=l"(w3) : "l"(c));
         k.f000 = __int_as_float(int(w0 & 0xffffffffull)); k.f100 = __int_as_float(int(w0 >> 32));
         k.f010 = __int_as_float(int(w1 & 0xffffffffull)); k.f110 = __int_as_float(int(w1 >> 32));
         k.f001 = __int_as_float(int(w2 & 0xffffffffull)); k.f101 = __int_as_float(int(w2 >> 32));
