@@ -100,6 +100,14 @@ typedef struct {
                                  (--rilc_bfgs 0, kernel2.cu:427-563): heuristic
                                  depth x 2.4 and (25 + atoms)/3 steps,
                                  main.cpp:367-389                           */
+    int32_t  visited_history; /* 1 = QuickVina2-CUDA's visited history
+                                 (QuickVina2-CUDA/inc/cuda/visited.cuh:48-227,
+                                 quasi_newton.cuh:1937-1943), RILC-BFGS only:
+                                 its novelty check returns false on every
+                                 path, so each chain runs its first
+                                 10 x (6 + ntors) local optimisations and
+                                 keeps every later candidate unoptimised at
+                                 its entry energy; 0 = off (Vina-CUDA)       */
 } vd_search_params;
 
 typedef struct {

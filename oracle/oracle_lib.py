@@ -109,7 +109,7 @@ class OrSearch(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("lig_uid", C.c_uint32), ("search_depth", C.c_int32),
                 ("max_bfgs_steps", C.c_int32), ("hunt_cap", C.c_double * 3),
                 ("slope", C.c_double), ("temperature", C.c_double), ("amplitude", C.c_double),
-                ("dense", C.c_int32)]
+                ("dense", C.c_int32), ("visited", C.c_int32)]
 
 
 class Oracle:
@@ -259,7 +259,8 @@ class Oracle:
         return c.copy()
 
     def mc_chains(self, lig, seed, lig_uid, depth, bfgs_steps, chain_begin, chain_end,
-                  threads=1, hunt_cap=(10, 10, 10), slope=1e6, temperature=1.2, amplitude=2.0, dense=False):
+                  threads=1, hunt_cap=(10, 10, 10), slope=1e6, temperature=1.2, amplitude=2.0, dense=False,
+                  visited=False):
         self._need_maps(lig)
         s = OrSearch()
         s.seed, s.lig_uid, s.search_depth, s.max_bfgs_steps = seed, lig_uid, depth, bfgs_steps
@@ -267,6 +268,7 @@ class Oracle:
             s.hunt_cap[i] = hunt_cap[i]
         s.slope, s.temperature, s.amplitude = slope, temperature, amplitude
         s.dense = int(bool(dense))
+        s.visited = int(bool(visited))
         n = chain_end - chain_begin
         nc = 7 + self.ntors[lig]
         conf, cp = _d(np.zeros(n * nc))

@@ -924,14 +924,28 @@ double mc_chain(const or_ctx* c, const Lig& L, const or_search& s, uint32_t chai
     }
     const int nc = 7 + L.ntors();
     Objective obj{c, &L, s.hunt_cap, s.slope, eval_deriv_cache};
-    std::vector<double> tmp(nc), cand(nc);
+    std::vector<double> tmp(nc), cand(nc), g(6 + L.ntors());
     init_conf(c, L, s.seed, s.lig_uid, chain, tmp.data());
     double tmp_e = kMax, best_e = std::numeric_limits<double>::infinity();
     std::memcpy(best, tmp.data(), sizeof(double) * nc);
+    // QuickVina2-CUDA's visited history (visited.cuh:48-227): rilc_bfgs_update
+    // evaluates the entry pose, and unless interesting() holds returns it with
+    // that energy (quasi_newton.cuh:1937-1943); interesting() is true until the
+    // history holds 10*(6+ntors) entries (one add() per optimisation run) and
+    // then consults check(), which returns false on every path
+    // (visited.cuh:91-166).  So a chain runs its first 10*(6+ntors)
+    // optimisations and keeps every later candidate's entry energy.
+    const int history = 10 * (6 + L.ntors());
+    int runs = 0;
+    auto local_search = [&](double* x) {
+        if (s.visited && runs >= history) return obj(x, g.data());
+        ++runs;
+        return rilc_bfgs(obj, L.ntors(), x, s.max_bfgs_steps);
+    };
     for (int step = 0; step < s.search_depth; ++step) {
         cand = tmp;
         mutate(L, cand.data(), s.seed, s.lig_uid, chain, uint32_t(step), s.amplitude, obj.F);
-        double ce = rilc_bfgs(obj, L.ntors(), cand.data(), s.max_bfgs_steps);
+        double ce = local_search(cand.data());
         Draw b(s.seed, s.lig_uid, chain, uint32_t(step), 1);
         bool acc = step == 0 || ce < tmp_e ||
                    u01(b.u[1]) < std::exp((tmp_e - ce) / s.temperature);  // kernel2.cu:63-71
@@ -939,7 +953,7 @@ double mc_chain(const or_ctx* c, const Lig& L, const or_search& s, uint32_t chai
             tmp = cand;
             tmp_e = ce;
             if (tmp_e < best_e) {
-                tmp_e = rilc_bfgs(obj, L.ntors(), tmp.data(), s.max_bfgs_steps);
+                tmp_e = local_search(tmp.data());
                 if (tmp_e < best_e) {
                     best_e = tmp_e;
                     std::memcpy(best, tmp.data(), sizeof(double) * nc);

@@ -92,6 +92,11 @@ typedef struct {
     double   amplitude;      /* 2                                           */
     int32_t  dense;          /* 0: RILC-BFGS local search (--rilc_bfgs 1);
                                 1: dense BFGS (--rilc_bfgs 0)               */
+    int32_t  visited;        /* 1: QuickVina2-CUDA's visited history (RILC
+                                only): a chain runs its first 10*(6+ntors)
+                                local optimisations, later candidates keep
+                                their entry energy (visited.cuh:48-227,
+                                quasi_newton.cuh:1937-1943)                  */
 } or_search;
 
 /* Runs chains [chain_begin, chain_end) of the Monte-Carlo search

@@ -168,6 +168,37 @@ def test_local_opt_matches_oracle_rilc(vd):
     assert ks_2samp(e_gpu, e_ref).pvalue >= 0.01
 
 
+def test_visited_history_matches_oracle(vd):
+    """QuickVina2-CUDA's visited history (vd_search_params.visited_history;
+    QuickVina2-CUDA/inc/cuda/visited.cuh:48-227, quasi_newton.cuh:1937-1943)
+    on a 1-torsion ligand: its history holds 10 x (6 + 1) = 70 optimiser runs,
+    and 150 Monte-Carlo steps run well past it, after which every candidate
+    keeps its entry energy.  GPU chains against the oracle's restatement of
+    the same policy on the same Philox streams, 512 chains: paired median
+    difference within 0.05 kcal/mol, two-sample KS p >= 0.01, evaluation
+    totals within 5%; the policy's skipped calls (one evaluation each) make
+    the search cheaper than the same search without it; each returned energy
+    is its pose's energy."""
+    from scipy.stats import ks_2samp
+    ctx, orc, lig, lc, lo = make_ligand_ctx(vd, n_atoms=12, n_tors=1, seed=29, box=16.0)
+    assert ctx.ntors[lc] == 1
+    n, depth, steps = 512, 150, 10
+    sp = vd.search_params(seed=5, n_chains=n, search_depth=depth, max_bfgs_steps=steps, visited_history=1)
+    p_gpu, e_gpu, ev = ctx.mc_chains(lc, sp)
+    _, _, ev_off = ctx.mc_chains(lc, vd.search_params(seed=5, n_chains=n, search_depth=depth, max_bfgs_steps=steps))
+    conf, e_ref, ev_ref = orc.mc_chains(lo, 5, lc, depth, steps, 0, n, threads=O_THREADS, visited=True)
+    for i in range(0, n, 64):
+        assert_pose_energy(ctx, orc, lig, lc, lo, p_gpu[i], e_gpu[i])
+    st = _chain_stats(e_gpu, e_ref)
+    print(f"visited history: {st}, evals gpu {ev} oracle {ev_ref}, without the history {ev_off}")
+    assert abs(st["paired_median"]) <= 0.05, st
+    assert st["ks_p"] >= 0.01, st
+    assert abs(ev - ev_ref) <= 0.05 * ev_ref, (ev, ev_ref)
+    assert ev < 0.9 * ev_off, (ev, ev_off)
+    with pytest.raises(vd.VdockError):
+        ctx.mc_chains(lc, vd.search_params(seed=5, n_chains=8, search_depth=2, dense_bfgs=1, visited_history=1))
+
+
 def test_mc_initial_poses_share_streams_with_oracle(vd):
     """A negative search_depth returns each chain's initial pose: the Philox draws
     (position in the box, normalised 4-D Gaussian rotation, torsions) are

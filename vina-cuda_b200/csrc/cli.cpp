@@ -124,6 +124,7 @@ static const char* kUsage =
     "  --weight_hydrogen --weight_rot\n"
     "Misc:\n  --seed arg  --num_modes arg (9)  --energy_range arg (3)  --device arg (0)\n"
     "  --batch arg (ligands per batched launch, 64)\n"
+    "  --visited_history arg (0; 1 = QuickVina2-CUDA's visited history, with --rilc_bfgs 1)\n"
     "Configuration file:\n  --config arg   (key = value lines with the options above)\n";
 
 int main(int argc, char** argv) {
@@ -168,6 +169,9 @@ int main(int argc, char** argv) {
     if (opt.count("search_depth") && search_depth < 1) die("search_depth must be 1 or greater");
     const int rilc_bfgs = int(num("rilc_bfgs", 1));  // main.cpp:663: 1 = RILC-BFGS, 0 = dense BFGS
     if (rilc_bfgs != 0 && rilc_bfgs != 1) die("rilc_bfgs must be 0 or 1");
+    const int visited = int(num("visited_history", 0));  // QuickVina2-CUDA's search policy
+    if (visited != 0 && visited != 1) die("visited_history must be 0 or 1");
+    if (visited && !rilc_bfgs) die("visited_history needs --rilc_bfgs 1");
     const double w_rot = num("weight_rot", 0.05846);
     const double weights[6] = {num("weight_gauss1", -0.035579), num("weight_gauss2", -0.005156),
                                num("weight_repulsion", 0.840245), num("weight_hydrophobic", -0.035069),
@@ -250,6 +254,7 @@ int main(int argc, char** argv) {
     sp.min_rmsd = 1.0;
     sp.refine = 1;
     sp.dense_bfgs = rilc_bfgs == 0;
+    sp.visited_history = visited;
     FILE* log = opt.count("log") ? std::fopen(opt["log"].c_str(), "w") : nullptr;
 
     struct Item {

@@ -48,6 +48,7 @@ struct DockParams {
     unsigned long long* lig_evals;  // [n_ligs] evaluations per ligand
     int32_t warp_floats;
     int32_t warps_per_block;
+    int32_t visited;             // QuickVina2-CUDA's visited history (RILC-BFGS only)
 };
 
 __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int item) {
@@ -70,7 +71,7 @@ __device__ __forceinline__ int find_ligand(const int32_t* prefix, int n, int ite
 // then (dense BFGS) the inverse Hessian and four pose-space vectors
 // (dense_floats).
 // chain scalar slots (ints, then floats)
-enum : int { kCsItem, kCsLig, kCsChain, kCsUid, kCsDepth, kCsSteps, kCsEvals0, kCsStep, kCsFloats };
+enum : int { kCsItem, kCsLig, kCsChain, kCsUid, kCsDepth, kCsSteps, kCsEvals0, kCsStep, kCsRuns, kCsFloats };
 enum : int { kCfCurrent, kCfBest };
 static_assert(kCsFloats + kCfBest + 1 <= kChainWords, "chain scalars exceed their shared words");
 
@@ -111,6 +112,7 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
             cs[kCsDepth] = __ldg(&p.depth[li0]);
             cs[kCsSteps] = __ldg(&p.bfgs_steps[li0]);
             cs[kCsEvals0] = evals;
+            cs[kCsRuns] = 0;
             cf[kCfCurrent] = FLT_MAX;
             cf[kCfBest] = INFINITY;
         }
@@ -138,7 +140,15 @@ __global__ void __launch_bounds__(128, MINB) dock_kernel(DockParams p) {
                     ce = dense_bfgs<true>(L, s, H, gc, pv, yv, mhy, gi, p.smooth, p.ep.v_intra, p.ep.fix,
                                           p.ep.inv_fix, cs[kCsSteps], lane, evals);
                 } else {
-                    ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, cs[kCsSteps], lane, evals);
+                    // visited history (visited.cuh:48-227, quasi_newton.cuh:1937-1943):
+                    // interesting() holds until 10 x (6 + ntors) runs have been
+                    // added to the history, then check() returns false on every
+                    // path, so later calls keep the candidate at its entry energy
+                    const int runs = cs[kCsRuns];
+                    const bool skip = p.visited && runs >= 10 * (6 + L.nt);
+                    __syncwarp();
+                    if (lane == 0 && !skip) cs[kCsRuns] = runs + 1;
+                    ce = rilc_bfgs(L, s, p.G, p.smooth, p.ep, cs[kCsSteps], lane, evals, skip);
                 }
                 const int stp = cs[kCsStep];
                 float tmp_e = cf[kCfCurrent], best_e = cf[kCfBest];
@@ -265,6 +275,8 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
                        DockBuffers& out) {
     VD_CHECK(!ligs.empty(), VD_ERR_ARG, "no ligands");
     VD_CHECK(sp.n_chains > 0, VD_ERR_ARG, "n_chains must be positive");
+    VD_CHECK(sp.visited_history == 0 || (sp.visited_history == 1 && !sp.dense_bfgs), VD_ERR_ARG,
+             "visited_history must be 0, or 1 with RILC-BFGS (QuickVina2-CUDA has no dense-BFGS search)");
     VD_CHECK(int64_t(ligs.size()) * sp.n_chains <= (int64_t(1) << 30), VD_ERR_CAPACITY,
              "more than 2^30 (ligand, chain) work items in one call");
     VD_CHECK(c.has_box, VD_ERR_ARG, "no box set");
@@ -346,6 +358,7 @@ vd_status prepare_dock(Ctx& c, const std::vector<int>& ligs, const vd_search_par
     p.evals = reinterpret_cast<unsigned long long*>(c.d_counter + 2);
     p.lig_evals = out.d_lig_evals;
     p.warp_floats = max_wf;
+    p.visited = sp.visited_history;
     // launch shape: register budget from the caller or the autotuner, keyed
     // by form, work items and shared memory per chain
     const int wpb = 4;
@@ -488,6 +501,8 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     Ctx& c = h->c;
     VD_CHECK(lig >= 0 && lig < int(c.ligs.size()), VD_ERR_ARG, "vd_mc_chains_noalloc: bad ligand id");
     VD_CHECK(sp->n_chains > 0, VD_ERR_ARG, "vd_mc_chains_noalloc: n_chains must be positive");
+    VD_CHECK(sp->visited_history == 0 || (sp->visited_history == 1 && !sp->dense_bfgs), VD_ERR_ARG,
+             "vd_mc_chains_noalloc: visited_history must be 0, or 1 with RILC-BFGS");
     VD_CHECK(c.has_box, VD_ERR_ARG, "vd_mc_chains_noalloc: no box set");
     VD_CHECK(!c.pool_dirty && c.d_pool, VD_ERR_ARG,
              "vd_mc_chains_noalloc: ligands not on the device yet; make one allocating call "
@@ -551,6 +566,7 @@ extern "C" vd_status vd_mc_chains_noalloc(vd_ctx* h, int32_t lig, const vd_searc
     p.stride = nc;
     p.out_e = d_e;
     p.queue = nullptr;  // one warp per chain: no work queue
+    p.visited = sp->visited_history;
     p.evals = d_cnt;
     p.lig_evals = d_cnt + 1;
     p.warp_floats = lig_warp_floats(L) + 4 * pad4(nc) + kChainWords + (sp->dense_bfgs ? dense_floats(L.h.ntors) : 0);

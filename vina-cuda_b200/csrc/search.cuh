@@ -145,8 +145,11 @@ struct SearchMem {  // per-warp shared memory of the optimiser
 // instruction caches better.  The operations and their order are those of
 // the straight-line form: entry evaluation, then per iteration a line search
 // (start, trials) and the direction update.
+// entry_only: evaluate the entry pose and return its energy without
+// optimising it (the visited-history policy's skipped calls,
+// quasi_newton.cuh:1937-1939).
 __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const MapView& G, const float4* smooth,
-                           const EvalParams ep, int max_steps, int lane, int& evals) {
+                           const EvalParams ep, int max_steps, int lane, int& evals, bool entry_only = false) {
     const int n = 6 + L.nt, nc = 7 + L.nt;
     if (max_steps <= 0) max_steps = 1000;  // the reference's 0 means unbounded
     float fx = 0.f, fx_orig = 0.f, fxp = 0.f, step = 0.f;
@@ -161,6 +164,7 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
         ++evals;
         g = vload(s.m.g, n, lane);
         if (first) {
+            if (entry_only) return fx;
             first = false;
             fx_orig = fx;
             copy_conf(s.m.x, s.xo, nc, lane);

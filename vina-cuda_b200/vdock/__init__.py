@@ -43,7 +43,7 @@ class SearchParams(C.Structure):
                 ("max_bfgs_steps", C.c_int32), ("num_modes", C.c_int32), ("energy_range", C.c_double),
                 ("hunt_cap", C.c_double * 3), ("temperature", C.c_double), ("amplitude", C.c_double),
                 ("min_rmsd", C.c_double), ("refine", C.c_int32), ("launch_shape", C.c_int32),
-                ("dense_bfgs", C.c_int32)]
+                ("dense_bfgs", C.c_int32), ("visited_history", C.c_int32)]
 
 
 class DockResult(C.Structure):
@@ -142,7 +142,7 @@ def _f(a):
 
 def search_params(seed=0, n_chains=8192, search_depth=0, max_bfgs_steps=0, num_modes=9,
                   energy_range=3.0, hunt_cap=(10, 10, 10), temperature=1.2, amplitude=2.0,
-                  min_rmsd=1.0, refine=1, launch_shape=0, dense_bfgs=0):
+                  min_rmsd=1.0, refine=1, launch_shape=0, dense_bfgs=0, visited_history=0):
     s = SearchParams()
     s.seed, s.n_chains, s.search_depth, s.max_bfgs_steps = seed, n_chains, search_depth, max_bfgs_steps
     s.num_modes, s.energy_range = num_modes, energy_range
@@ -151,6 +151,7 @@ def search_params(seed=0, n_chains=8192, search_depth=0, max_bfgs_steps=0, num_m
     s.temperature, s.amplitude, s.min_rmsd, s.refine = temperature, amplitude, min_rmsd, refine
     s.launch_shape = launch_shape
     s.dense_bfgs = int(dense_bfgs)
+    s.visited_history = int(visited_history)
     return s
 
 
