@@ -17,10 +17,12 @@ pytestmark = pytest.mark.gpu
 CLI = os.environ.get("VDOCK_CLI") or os.path.join(REPO, "vina-cuda_b200", "vdock_cli")
 
 
-@pytest.mark.parametrize("rilc_bfgs", [1, 0])
-def test_cli_docks_reference_example(tmp_path, golden_dir, rilc_bfgs):
+@pytest.mark.parametrize("rilc_bfgs,visited", [(1, 0), (0, 0), (1, 1)], ids=["rilc", "dense", "visited"])
+def test_cli_docks_reference_example(tmp_path, golden_dir, rilc_bfgs, visited):
     """Both local searches of the reference's --rilc_bfgs option (main.cpp:663):
-    1 = RILC-BFGS, 0 = dense BFGS with its own depth and step heuristics."""
+    1 = RILC-BFGS, 0 = dense BFGS with its own depth and step heuristics; and
+    RILC-BFGS with QuickVina2-CUDA's visited history (--visited_history 1),
+    which the heuristic depth never fills."""
     if not has_gpu():
         pytest.skip("needs a CUDA device")
     cli = CLI
@@ -31,7 +33,7 @@ def test_cli_docks_reference_example(tmp_path, golden_dir, rilc_bfgs):
     cfg = (tmp_path / "1u1b_config.txt").read_text()
     lines = [l for l in cfg.splitlines() if not l.strip().startswith(("receptor", "ligand", "out", "thread"))]
     lines += ["receptor = 1u1b_protein.pdbqt", "ligand = 1u1b_ligand.pdbqt", "out = out.pdbqt", "thread = 8192",
-              "seed = 7", f"rilc_bfgs = {rilc_bfgs}"]
+              "seed = 7", f"rilc_bfgs = {rilc_bfgs}", f"visited_history = {visited}"]
     (tmp_path / "cfg.txt").write_text("\n".join(lines) + "\n")
     r = subprocess.run([cli, "--config", "cfg.txt"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
@@ -42,6 +44,10 @@ def test_cli_docks_reference_example(tmp_path, golden_dir, rilc_bfgs):
     best = float(remarks[0].split()[3])
     assert -9.5 <= best <= -6.5, best
     assert "mode |   affinity" in r.stdout
+    if visited:  # QuickVina2-CUDA has no dense-BFGS search: the combination is refused
+        bad = subprocess.run([cli, "--config", "cfg.txt", "--rilc_bfgs", "0"], cwd=tmp_path, capture_output=True,
+                             text=True, timeout=600)
+        assert bad.returncode != 0 and "visited_history" in bad.stderr
 
 
 def test_cli_ligand_directory(tmp_path, golden_dir):
