@@ -532,14 +532,15 @@ def run_ours(a):
         "host_and_gaps_ms_per_ligand": 1e3 * elapsed / (K * B) - (dock_ms + post_ms) / (K * B),
         "dock_kernel_evals_per_s": evals / (dock_ms / 1e3)}
     # end to end through the public API with host buffers: ligand topologies
-    # copied in (vd_add_ligand + pool upload), results read back
+    # copied in (vd_add_ligands, which packs the batch on host threads, + pool
+    # upload), results read back
     e2e_times, h2d_steps = [], []
     n_e2e = K if a.e2e_steps <= 0 else min(a.e2e_steps, K)
     for k in range(n_e2e):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx.clear_ligands()
-        eids = [ctx.add_ligand(ligs[lid]) for lid in batches[W + k]]
+        eids = ctx.add_ligands([ligs[lid] for lid in batches[W + k]])
         res = ctx.dock_batched(eids, sp)
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)

@@ -186,6 +186,12 @@ vd_status vd_get_grid(vd_ctx* ctx, int32_t xs_type, float* out);
 
 /* ---- ligands -------------------------------------------------------------- */
 vd_status vd_add_ligand(vd_ctx* ctx, const vd_ligand_desc* lig, int32_t* lig_id);
+/* n ligands at once (the per-ligand packing of main_procedure_cu.cpp:550-846
+ * for a whole list): the blobs, pair segments and search schedules are built
+ * on up to 32 host threads, then appended in list order, so lig_ids and
+ * every later result equal n vd_add_ligand calls.  If a descriptor is
+ * invalid, none is added and the error names its index. */
+vd_status vd_add_ligands(vd_ctx* ctx, const vd_ligand_desc* ligs, int32_t n, int32_t* lig_ids);
 vd_status vd_ligand_info(vd_ctx* ctx, int32_t lig_id, int32_t* n_heavy, int32_t* ntors,
                          int32_t* n_pairs);
 vd_status vd_clear_ligands(vd_ctx* ctx);

@@ -283,6 +283,32 @@ def test_plain_and_batched_forms_compute_identical_chains(vd):
     np.testing.assert_array_equal(r_plain["pose"], r_batch["pose"])
 
 
+def test_batch_add_equals_single_adds(vd):
+    """vd_add_ligands (the list packed on host threads) gives the ids, blobs
+    and docking results of one vd_add_ligand call per ligand; with an invalid
+    descriptor in the list it adds none and names the ligand."""
+    from vdock import synth
+    ligs = synth.ligand_set(40, (10, 60), (0, 15), seed=41)
+    sp = vd.search_params(seed=3, n_chains=16, search_depth=3, max_bfgs_steps=10, refine=1)
+    res = []
+    for batch in (False, True):
+        ctx, _, _, _, _ = make_ligand_ctx(vd, n_atoms=18, n_tors=3, seed=19)
+        ctx.build_grids(synth.TYPES8)
+        ids = ctx.add_ligands(ligs) if batch else [ctx.add_ligand(l) for l in ligs]
+        assert ids == list(range(1, 41)), ids
+        res.append(ctx.dock_batched(ids, sp))
+        if batch:
+            bad = dict(ligs[7])
+            bad["atom_node"] = np.full_like(np.asarray(bad["atom_node"]), 99)
+            with pytest.raises(vd.VdockError, match="ligand 1"):
+                ctx.add_ligands([ligs[3], bad, ligs[5]])
+            assert ctx.add_ligand(ligs[0]) == 41  # nothing of the failed list was added
+        ctx.close()
+    for a, b in zip(*res):
+        np.testing.assert_array_equal(a["energy"], b["energy"])
+        np.testing.assert_array_equal(a["pose"], b["pose"])
+
+
 def test_score_matches_oracle_eval_adjusted(vd):
     """vd_score (FP64 rescoring on the direct-sum score) equals the oracle's
     eval_adjusted (model.cpp:1428-1431) and eval_intramolecular

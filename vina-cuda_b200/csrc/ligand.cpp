@@ -3,6 +3,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
+#include <thread>
 
 #include "common.h"
 #include "schedule.h"
@@ -85,16 +87,10 @@ std::vector<int2> order_pairs(const std::vector<int2>& in) {
     return out;
 }
 
-}  // namespace
-}  // namespace vd
-
-using namespace vd;
-
-extern "C" {
-
-vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
-    VD_CHECK(h && d && lig_id, VD_ERR_ARG, "vd_add_ligand: NULL argument");
-    Ctx& c = h->c;
+// Validates one ligand descriptor and builds its device blob and host
+// copies; touches no context state, so ligands can be built concurrently.
+vd_status build_ligand(const vd_ligand_desc* d, HostLigand& L) {
+    VD_CHECK(d, VD_ERR_ARG, "vd_add_ligand: NULL argument");
     const int na = d->n_atoms, nn = d->n_nodes, np = d->n_pairs;
     VD_CHECK(na >= 1 && nn >= 1 && np >= 0, VD_ERR_ARG, "vd_add_ligand: empty ligand");
     VD_CHECK(d->xyz && d->xs && d->el && d->atom_node && d->node_parent && d->node_origin_atom &&
@@ -201,7 +197,7 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
         nodes[k].atom_end = hb[k + 1];
         nodes[k].sub_atom_end = hb[sub_end[k]];
     }
-    HostLigand L;
+    L = HostLigand{};
     LigHeader& H = L.h;
     std::memset(&H, 0, sizeof(H));
     H.n_atoms = nh;
@@ -258,11 +254,61 @@ vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
     L.heavy_index = heavy_index;
     L.n_all_atoms = na;
     L.num_tors = d->num_tors;
+    return VD_OK;
+}
+
+// Appends a built ligand to the context's pool (its blob's offset is fixed
+// here; the next docking call uploads it).
+int32_t append_ligand(Ctx& c, HostLigand&& L) {
     L.pool_offset = c.pool_words;
     c.pool_words += int64_t(L.blob.size());
     c.ligs.push_back(std::move(L));
     c.pool_dirty = true;
-    *lig_id = int32_t(c.ligs.size()) - 1;
+    return int32_t(c.ligs.size()) - 1;
+}
+
+}  // namespace
+}  // namespace vd
+
+using namespace vd;
+
+extern "C" {
+
+vd_status vd_add_ligand(vd_ctx* h, const vd_ligand_desc* d, int32_t* lig_id) {
+    VD_CHECK(h && d && lig_id, VD_ERR_ARG, "vd_add_ligand: NULL argument");
+    HostLigand L;
+    const vd_status st = build_ligand(d, L);
+    if (st != VD_OK) return st;
+    *lig_id = append_ligand(h->c, std::move(L));
+    return VD_OK;
+}
+
+vd_status vd_add_ligands(vd_ctx* h, const vd_ligand_desc* descs, int32_t n, int32_t* lig_ids) {
+    VD_CHECK(h && n >= 0 && (n == 0 || (descs && lig_ids)), VD_ERR_ARG, "vd_add_ligands: NULL argument");
+    std::vector<HostLigand> built(size_t(n) > 0 ? size_t(n) : 0);
+    std::vector<vd_status> status(built.size(), VD_OK);
+    std::vector<std::string> message(built.size());
+    const int hw = int(std::max(1u, std::thread::hardware_concurrency()));
+    const int workers = std::max(1, std::min({n, hw, 32}));
+    auto work = [&](int w) {
+        for (int i = w; i < n; i += workers) {  // interleaved: sizes vary along a list
+            status[i] = build_ligand(&descs[i], built[i]);
+            if (status[i] != VD_OK) message[i] = vd_last_error();  // this worker's message
+        }
+    };
+    if (workers == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int w = 0; w < workers; ++w) pool.emplace_back(work, w);
+        for (auto& t : pool) t.join();
+    }
+    for (int i = 0; i < n; ++i)
+        if (status[i] != VD_OK) {
+            set_error("vd_add_ligands: ligand " + std::to_string(i) + ": " + message[i]);
+            return status[i];
+        }
+    for (int i = 0; i < n; ++i) lig_ids[i] = append_ligand(h->c, std::move(built[i]));
     return VD_OK;
 }
 

@@ -63,7 +63,8 @@ class Stats(C.Structure):
 EXPORTS = [
     "vd_create", "vd_destroy", "vd_last_error", "vd_get_stats", "vd_set_memory_cap", "vd_set_scoring",
     "vd_set_scoring_device", "vd_set_receptor",
-    "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand", "vd_ligand_info",
+    "vd_set_box", "vd_grid_dims", "vd_build_grids", "vd_set_grid_shape", "vd_get_grid", "vd_add_ligand",
+    "vd_add_ligands", "vd_ligand_info",
     "vd_clear_ligands", "vd_energy", "vd_energy_grad", "vd_energy_grad_device", "vd_energy_device",
     "vd_pose_coords",
     "vd_local_opt", "vd_mc_chains", "vd_mc_chains_noalloc", "vd_dock_plain", "vd_dock_batched", "vd_refine", "vd_score",
@@ -92,6 +93,7 @@ def lib():
         L.vd_get_grid.argtypes = [_vp, C.c_int32, _fp]
         L.vd_set_grid_shape.argtypes = [_vp, C.c_int32]
         L.vd_add_ligand.argtypes = [_vp, C.POINTER(LigandDesc), _ip]
+        L.vd_add_ligands.argtypes = [_vp, C.POINTER(LigandDesc), C.c_int32, C.POINTER(C.c_int32)]
         L.vd_ligand_info.argtypes = [_vp, C.c_int32, _ip, _ip, _ip]
         L.vd_clear_ligands.argtypes = [_vp]
         L.vd_energy.argtypes = [_vp, C.c_int32, C.c_int32, _fp, C.POINTER(EvalParams), _fp]
@@ -241,9 +243,8 @@ class Context:
         _check(self.L.vd_get_grid(self.h, t, op))
         return out.reshape(n[2], n[1], n[0])
 
-    def add_ligand(self, desc):
-        keep = {}
-        s = LigandDesc()
+    @staticmethod
+    def _desc(desc, s, keep):
         s.n_atoms = int(desc["n_atoms"])
         s.n_nodes = int(len(desc["node_parent"]))
         s.n_pairs = int(len(desc["pairs"]))
@@ -252,14 +253,35 @@ class Context:
             keep[k], p = _i(desc[k])
             setattr(s, k, p)
         s.num_tors = float(desc["num_tors"])
-        lid = C.c_int32(-1)
-        _check(self.L.vd_add_ligand(self.h, C.byref(s), C.byref(lid)))
+
+    def _registered(self, lid, keep):
         nh, nt, npair = C.c_int32(), C.c_int32(), C.c_int32()
-        _check(self.L.vd_ligand_info(self.h, lid.value, C.byref(nh), C.byref(nt), C.byref(npair)))
+        _check(self.L.vd_ligand_info(self.h, lid, C.byref(nh), C.byref(nt), C.byref(npair)))
         self._keep.append(keep)
         self.ntors.append(nt.value)
         self.n_heavy.append(nh.value)
+
+    def add_ligand(self, desc):
+        keep = {}
+        s = LigandDesc()
+        self._desc(desc, s, keep)
+        lid = C.c_int32(-1)
+        _check(self.L.vd_add_ligand(self.h, C.byref(s), C.byref(lid)))
+        self._registered(lid.value, keep)
         return lid.value
+
+    def add_ligands(self, descs):
+        """vd_add_ligands: the list built on host threads, ids in list order."""
+        n = len(descs)
+        arr = (LigandDesc * max(n, 1))()
+        keeps = [{} for _ in range(n)]
+        for i, d in enumerate(descs):
+            self._desc(d, arr[i], keeps[i])
+        ids = (C.c_int32 * max(n, 1))()
+        _check(self.L.vd_add_ligands(self.h, arr, n, ids))
+        for i in range(n):
+            self._registered(ids[i], keeps[i])
+        return [ids[i] for i in range(n)]
 
     def clear_ligands(self):
         _check(self.L.vd_clear_ligands(self.h))
