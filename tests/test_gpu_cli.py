@@ -53,8 +53,9 @@ def test_cli_docks_reference_example(tmp_path, golden_dir, rilc_bfgs, visited):
 def test_cli_ligand_directory(tmp_path, golden_dir):
     """--ligand_directory: every file of the directory docked in batches while
     later files are still being parsed, outputs named <stem>_out.pdbqt in
-    --output_directory (main.cpp:897-945), unparsable files skipped with a
-    message, results independent of parse timing (two runs are identical)."""
+    --output_directory (main.cpp:897-945), unparsable files and ligands the
+    kernels cannot hold skipped with a message, results independent of parse
+    timing (two runs are identical)."""
     if not has_gpu():
         pytest.skip("needs a CUDA device")
     cli = CLI
@@ -69,6 +70,12 @@ def test_cli_ligand_directory(tmp_path, golden_dir):
         (ligdir / (name + ".pdbqt")).write_bytes(data)
         (ligdir / (name + "_copy.pdbqt")).write_bytes(data)
     (ligdir / "broken.pdbqt").write_text("ATOM  garbage\nBRANCH 1 2\n")
+    # parses, but 130 heavy atoms exceed the kernels' 128: its batch is packed
+    # one ligand at a time and this one skipped
+    grid = [(x, y, z) for x in range(6) for y in range(5) for z in range(5)][:130]
+    big = ["ROOT"] + [f"ATOM  {i + 1:5d}  C   LIG A   1    {1.5 * x:8.3f}{1.5 * y:8.3f}{1.5 * z:8.3f}"
+                      f"  0.00  0.00    +0.000 C " for i, (x, y, z) in enumerate(grid)] + ["ENDROOT", "TORSDOF 0"]
+    (ligdir / "big.pdbqt").write_text("\n".join(big) + "\n")
     cfg = (tmp_path / "1u1b_config.txt").read_text()
     lines = [l for l in cfg.splitlines() if not l.strip().startswith(("receptor", "ligand", "out", "thread"))]
     outputs = []
@@ -79,6 +86,7 @@ def test_cli_ligand_directory(tmp_path, golden_dir):
         r = subprocess.run([cli, "--config", "cfg.txt"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr
         assert "broken.pdbqt" in r.stderr  # reported and skipped
+        assert "skipping" in r.stderr and "big.pdbqt" in r.stderr and "128 heavy atoms" in r.stderr
         assert "Docked 6 ligands" in r.stdout
         outdir = tmp_path / f"out_{run}"
         files = sorted(p.name for p in outdir.iterdir())

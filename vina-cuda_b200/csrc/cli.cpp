@@ -265,8 +265,28 @@ int main(int argc, char** argv) {
     std::vector<Item> pending;
     size_t n_docked = 0;
     auto run_batch = [&]() {
-        std::vector<int32_t> ids;
-        for (auto& it : pending) ids.push_back(it.id);
+        // the batch's ligands are packed together on host threads; if one is
+        // rejected, they are added one by one and the rejected ones skipped
+        std::vector<vd_ligand_desc> descs;
+        for (auto& it : pending) descs.push_back(it.s.d);
+        std::vector<int32_t> ids(pending.size());
+        if (vd_add_ligands(ctx, descs.data(), int32_t(descs.size()), ids.data()) != VD_OK) {
+            std::vector<Item> kept;
+            ids.clear();
+            for (auto& it : pending) {
+                if (vd_add_ligand(ctx, &it.s.d, &it.id) != VD_OK) {
+                    std::fprintf(stderr, "skipping %s: %s\n", ligs[it.file].c_str(), vd_last_error());
+                    vd_pdbqt_free(it.s.h);
+                    continue;
+                }
+                kept.push_back(it);
+                ids.push_back(it.id);
+            }
+            pending.swap(kept);
+            if (pending.empty()) return;
+        } else {
+            for (size_t k = 0; k < pending.size(); ++k) pending[k].id = ids[k];
+        }
         std::vector<vd_dock_result> res(ids.size());
         if (ids.size() == 1) check(vd_dock_plain(ctx, ids[0], &sp, &res[0]), "vd_dock_plain");
         else check(vd_dock_batched(ctx, ids.data(), int32_t(ids.size()), &sp, res.data()), "vd_dock_batched");
@@ -309,13 +329,7 @@ int main(int argc, char** argv) {
             std::fprintf(stderr, "\nParse error in file \"%s\": %s\n", ligs[i].c_str(), s.err.c_str());
             continue;
         }
-        int32_t id = -1;
-        if (vd_add_ligand(ctx, &s.d, &id) != VD_OK) {
-            std::fprintf(stderr, "skipping %s: %s\n", ligs[i].c_str(), vd_last_error());
-            vd_pdbqt_free(s.h);
-            continue;
-        }
-        pending.push_back({i, s, id});
+        pending.push_back({i, s, -1});  // added with the rest of its batch
         if (int(pending.size()) == batch) run_batch();
     }
     if (!pending.empty()) run_batch();
