@@ -126,9 +126,9 @@ def lig_bytes(lig):
 # DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
 # captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
 # ligands x 6,500 chains, 11.55 M evaluations per launch): 80 registers
-# 5.58 GB per launch.  The bench scales the figure by the evaluations of
+# 5.50 GB per launch.  The bench scales the figure by the evaluations of
 # each launch; shapes not captured report no traffic.
-DOCK_DRAM_BYTES_PER_EVAL = {4: 482.7}
+DOCK_DRAM_BYTES_PER_EVAL = {4: 477.6}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 # L1 data-pipe (LSU) wavefronts of one grid build of this workload (188^3
 # points x 8 maps, 8,000-atom receptor), from the ncu capture summarised in
