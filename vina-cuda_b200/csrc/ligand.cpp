@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <system_error>
 #include <thread>
 
 #include "common.h"
@@ -299,8 +300,17 @@ vd_status vd_add_ligands(vd_ctx* h, const vd_ligand_desc* descs, int32_t n, int3
     if (workers == 1) {
         work(0);
     } else {
+        // threads that cannot be started leave their share to this thread
         std::vector<std::thread> pool;
-        for (int w = 0; w < workers; ++w) pool.emplace_back(work, w);
+        std::vector<int> unstarted;
+        for (int w = 0; w < workers; ++w) {
+            try {
+                pool.emplace_back(work, w);
+            } catch (const std::system_error&) {
+                unstarted.push_back(w);
+            }
+        }
+        for (int w : unstarted) work(w);
         for (auto& t : pool) t.join();
     }
     for (int i = 0; i < n; ++i)
