@@ -313,9 +313,14 @@ def test_reference_example_docked_over_seeds(vd):
     search from an unrecorded seed, so the check is distributional: the
     reference's mode-1 score (+-0.05 print rounding) lies within the range of
     our 16 best scores and within 2 of their standard deviations of their
-    median.  The top poses' RMSD to the reference's mode 1 is reported: most
-    runs end in a site ~9.5 A away that scores better than the reference's
-    mode 1 under the same FP64 rescoring (-8.3 to -8.6 kcal/mol)."""
+    median.  The oracle's restatement of the reference's search and pipeline
+    (tests/pipeline_ref.py) docks the same example with the first 8 seeds:
+    the reference's score lies within its range too, and the GPU's and the
+    oracle's best-score distributions agree (two-sample KS p >= 0.01, medians
+    within 3 standard errors of their difference).  The top poses' RMSD to
+    the reference's mode 1 is reported: most runs end in a site ~9.5 A away
+    that scores better than the reference's mode 1 under the same FP64
+    rescoring (-8.3 to -8.6 kcal/mol)."""
     import kat_fit
     z = kat_fit.load()
     names = [str(n) for n in z["names"]]
@@ -342,6 +347,23 @@ def test_reference_example_docked_over_seeds(vd):
           f"{np.round(rms, 2).tolist()}")
     assert best.min() - 0.05 <= e_ref <= best.max() + 0.05, (e_ref, best)
     assert abs(e_ref - med) <= 2 * sd + 0.05, (e_ref, med, sd)
+    from scipy.stats import ks_2samp
+    from pipeline_ref import heuristics, oracle_dock
+    orc = O.Oracle()
+    orc.set_receptor(z["rec_xyz"], z["rec_xs"])
+    orc.set_box(z["center"], z["size"])
+    orc.build_grids(sorted(set(int(t) for t in d["xs"] if t >= 0)))
+    lo = orc.add_ligand(d)
+    depth, steps = heuristics(int(d["n_atoms"]), ctx.ntors[lid])
+    ob = np.array([oracle_dock(orc, lo, lid, 1000 + k, depth, steps, 8192)[0][0] for k in range(8)])
+    iqr = lambda v: float(np.subtract(*np.percentile(v, [75, 25])))
+    se = 1.2533 * np.hypot(iqr(best) / np.sqrt(len(best)), iqr(ob) / np.sqrt(len(ob))) / 1.349
+    print(f"reference example, oracle over 8 seeds: median {np.median(ob):.3f} range [{ob.min():.3f}, "
+          f"{ob.max():.3f}]; GPU - oracle medians {med - np.median(ob):.3f} (se {se:.3f}), "
+          f"KS p {ks_2samp(best, ob).pvalue:.3g}")
+    assert ob.min() - 0.05 <= e_ref <= ob.max() + 0.05, (e_ref, ob)
+    assert ks_2samp(best, ob).pvalue >= 0.01, (best, ob)
+    assert abs(med - np.median(ob)) <= 3 * se, (med, np.median(ob), se)
 
 
 def test_reference_docked_outputs_rescored_on_gpu(vd):
