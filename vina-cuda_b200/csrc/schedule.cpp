@@ -162,7 +162,10 @@ void refine_round(std::vector<int2>& r, uint64_t seed) {
         x = x * 6364136223846793005ull + 1442695040888963407ull;
         return uint32_t(x >> 33);
     };
-    constexpr int kMoves = 1500, kStall = 200;
+    // 1,500 moves: measured against 200-move stalls (lighter host work,
+    // coordinate-load conflicts 7% higher) and 4,000 moves (3x the host work
+    // for 1% fewer); ligand lists are packed on host threads (vd_add_ligands)
+    constexpr int kMoves = 1500, kStall = 1500;
     long best = L.cost;
     for (int it = 0, stall = 0; it < kMoves && stall < kStall; ++it, ++stall) {
         if (L.cost < best) { best = L.cost; stall = 0; }
