@@ -257,3 +257,33 @@ def test_fitted_poses_reproduce_reference_remarks():
             assert abs(lb - lb_ref) <= 0.0015 and abs(ub - ub_ref) <= 0.0015, (z["names"][i], lb, ub)
             n += 1
     assert n == 342
+
+
+def test_visited_history_policy_in_the_oracle():
+    """The oracle's restatement of QuickVina2-CUDA's visited history
+    (visited.cuh:48-227, quasi_newton.cuh:1937-1943): below its limit of
+    10 x (6 + ntors) optimiser runs per chain it changes nothing (identical
+    chains with and without it); past the limit every later candidate keeps
+    its entry energy at one evaluation, so a long search costs fewer
+    evaluations, and each chain's returned energy is its pose's energy."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "vina-cuda_b200"))
+    from vdock import synth
+    xyz, xs = synth.receptor(400, 14.0, seed=3)
+    lig = synth.ligand(9, 1, seed=4)
+    o = O.Oracle()
+    o.set_receptor(xyz, xs)
+    o.set_box([0, 0, 0], [12.0, 12.0, 12.0])
+    o.build_grids(sorted(set(int(t) for t in lig["xs"])))
+    lo = o.add_ligand(lig)
+    nt = o.ntors[lo]
+    assert nt == 1  # history limit 70 runs
+    short = [o.mc_chains(lo, 9, 0, 20, 8, 0, 6, visited=v) for v in (False, True)]
+    np.testing.assert_array_equal(short[0][0], short[1][0])
+    np.testing.assert_array_equal(short[0][1], short[1][1])
+    assert short[0][2] == short[1][2]
+    off = o.mc_chains(lo, 9, 0, 150, 8, 0, 6, visited=False)
+    on = o.mc_chains(lo, 9, 0, 150, 8, 0, 6, visited=True)
+    assert on[2] < 0.8 * off[2], (on[2], off[2])
+    for conf, e in zip(on[0], on[1]):
+        assert abs(o.eval_deriv(lo, conf)[0] - e) <= 1e-9 * max(1.0, abs(e))
