@@ -312,15 +312,31 @@ struct GridInter {
     }
 };
 
+// Adjoint-skip tests for eval_pose_t (below).  NoSkip: always compute it.
+struct NoSkip {
+    __device__ __forceinline__ bool operator()(float) const { return false; }
+};
+// Skip when the energy exceeds a threshold (+inf: never; a NaN energy never
+// exceeds it).
+struct SkipAbove {
+    float thr;
+    __device__ __forceinline__ bool operator()(float e) const { return e > thr; }
+};
+
 // pair_atomics: pairs from the search schedule, both atoms' forces by
 // atomics (no per-lane flush when the second atom changes: shorter, less
 // divergent code, which the latency-bound search prefers); otherwise the
 // second atom's force is summed in registers along b-sorted segments, which
 // the pose kernels, bound by L1 wavefronts, prefer (fewer atomics and
 // coordinate loads).
-template <bool want_grad, bool pair_atomics = false, class Inter>
+// skip(e): called with the energy (the same in every lane) once it is
+// known; when it returns true the adjoint phases (prefix sums, torques) are
+// skipped and m.g is left as it was.  The line searches pass a test that
+// holds exactly when the trial's gradient will not be read (a failed Armijo
+// test that is not the search's last trial).
+template <bool want_grad, bool pair_atomics = false, class Inter, class Skip = NoSkip>
 __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const Inter& inter, const float4* smooth,
-                             float v_intra, float fix, float inv_fix, int lane) {
+                             float v_intra, float fix, float inv_fix, int lane, const Skip& skip = Skip()) {
     frames(L, m, lane);
     float e = 0.f;
     // 3: per atom its coordinates (kept for the pair phase) and the grid
@@ -479,7 +495,7 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
         flush(-1);
     }
     e = warp_sum(e);
-    if (!want_grad) return e;
+    if (!want_grad || skip(e)) return e;
     __syncwarp();
     // 6: prefix sums over the heavy atoms of force and moment about the root
     // origin.  Atoms are grouped by body in pre-order, so a subtree's atoms
@@ -585,11 +601,12 @@ __device__ inline float eval_pose_t(const LigView& L, const WarpMem& m, const In
     return e;
 }
 
-template <bool want_grad, bool pair_atomics = false>
+template <bool want_grad, bool pair_atomics = false, class Skip = NoSkip>
 __device__ __forceinline__ float eval_pose(const LigView& L, const WarpMem& m, const MapView& G,
-                                           const float4* smooth, const EvalParams ep, int lane) {
+                                           const float4* smooth, const EvalParams ep, int lane,
+                                           const Skip& skip = Skip()) {
     const GridInter gi{&G, ep.v_inter, ep.slope};
-    return eval_pose_t<want_grad, pair_atomics>(L, m, gi, smooth, ep.v_intra, ep.fix, ep.inv_fix, lane);
+    return eval_pose_t<want_grad, pair_atomics>(L, m, gi, smooth, ep.v_intra, ep.fix, ep.inv_fix, lane, skip);
 }
 
 }  // namespace vd

@@ -160,7 +160,11 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
     float mu = 0.f, nu = 1.0e20f, finit = 0.f, dgtest = 0.f, dstest = 0.f;
     for (;;) {
         if (!first) conf_step(s.xp, s.m.x, d, step, L.nt, lane);  // the line search's trial pose
-        fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane);
+        // a trial that fails the Armijo test before the tenth reads no
+        // gradient: its adjoint is skipped
+        const float armijo = finit + step * dgtest;  // one value for the skip and the test below
+        fx = eval_pose<true, true>(L, s.m, G, smooth, ep, lane,
+                                   SkipAbove{(!first && count + 1 < 10) ? armijo : INFINITY});
         ++evals;
         g = vload(s.m.g, n, lane);
         if (first) {
@@ -175,7 +179,7 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
         } else {
             ++count;
             bool accept = false;
-            if (fx > finit + step * dgtest) {
+            if (fx > armijo) {
                 nu = step;
                 brackt = true;
             } else {
@@ -245,6 +249,14 @@ __device__ inline float rilc_bfgs(const LigView& L, const SearchMem& s, const Ma
     return fx;
 }
 
+// Adjoint skip of the dense line search: a trial whose Armijo test
+// (bfgs.h:72) fails.
+struct SkipArmijo {
+    float f0, c;
+    bool on;
+    __device__ __forceinline__ bool operator()(float e) const { return on && !(e - f0 < c); }
+};
+
 // bfgs.h:95-140 (dense BFGS, Armijo backtracking line_search 65-82,
 // bfgs_update 49-63) and its GPU form bfgs_optimized
 // (quasi_newton.cuh:2391-2499, line_search_optimized 1859-1916), warp-
@@ -269,7 +281,11 @@ __device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, floa
     bool first = true;
     for (;;) {
         if (!first) conf_step(s.xp, s.m.x, p, alpha, L.nt, lane);
-        const float fe = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane);
+        // a trial that fails the Armijo test before the tenth reads no
+        // gradient: its adjoint is skipped
+        const float armijo = 0.0001f * alpha * pg;
+        const float fe = eval_pose_t<true, pair_atomics>(L, s.m, inter, smooth, v_intra, fix, inv_fix, lane,
+                                                         SkipArmijo{f0, armijo, !first && trial + 1 < 10});
         ++evals;
         if (first) {
             first = false;
@@ -278,7 +294,7 @@ __device__ float dense_bfgs(const LigView& L, const SearchMem& s, float* H, floa
             f_orig = f0;
             copy_conf(s.m.x, s.xo, nc, lane);
         } else {
-            if (!(fe - f0 < 0.0001f * alpha * pg)) {  // line_search, bfgs.h:65-82
+            if (!(fe - f0 < armijo)) {  // line_search, bfgs.h:65-82
                 alpha *= 0.5f;
                 if (++trial < 10) continue;
             }
