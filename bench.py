@@ -126,9 +126,14 @@ def lig_bytes(lig):
 # DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
 # captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
 # ligands x 6,500 chains, 11.55 M evaluations per launch): 80 registers
-# 5.50 GB per launch.  The bench scales the figure by the evaluations of
+# 5.52 GB per launch.  The bench scales the figure by the evaluations of
 # each launch; shapes not captured report no traffic.
-DOCK_DRAM_BYTES_PER_EVAL = {4: 477.6}
+DOCK_DRAM_BYTES_PER_EVAL = {4: 477.4}
+# L1 data-pipe (LSU) wavefronts per evaluation of dock_kernel, per launch
+# shape, from the same capture (l1tex__data_pipe_lsu_wavefronts.sum over the
+# launch's evaluations): the kernel's limit is that pipe, one wavefront per
+# SM per cycle.  Shapes not captured report no fraction.
+DOCK_L1_WAVEFRONTS_PER_EVAL = {4: 462.7}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 # L1 data-pipe (LSU) wavefronts of one grid build of this workload (188^3
 # points x 8 maps, 8,000-atom receptor), from the ncu capture summarised in
@@ -151,6 +156,21 @@ def grid_l1_roof(ms, clk, device):
     peak = sms * mhz * 1e6  # wavefronts per second
     return {"l1_wavefronts": GRID_L1_WAVEFRONTS, "l1_wavefronts_per_s": GRID_L1_WAVEFRONTS / (ms / 1e3),
             "frac_of_l1_wavefront_roof": GRID_L1_WAVEFRONTS / (ms / 1e3) / peak}
+
+
+def dock_l1_roof(shape, evals, ms, clk, device):
+    """Fraction of the L1 data-pipe wavefront roof the docking kernel
+    reaches over the timed launches: ncu wavefronts per evaluation x the
+    evaluations timed / (kernel time x SMs x median SM clock x 1 wavefront
+    per SM per cycle)."""
+    if shape not in DOCK_L1_WAVEFRONTS_PER_EVAL:
+        return None
+    import torch
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clk.get("sm_mhz") or 1965.0
+    wf = DOCK_L1_WAVEFRONTS_PER_EVAL[shape] * evals
+    return {"wavefronts_per_eval": DOCK_L1_WAVEFRONTS_PER_EVAL[shape], "wavefronts_per_s": wf / (ms / 1e3),
+            "peak_per_s": sms * mhz * 1e6, "frac": wf / (ms / 1e3) / (sms * mhz * 1e6)}
 
 
 def peaks():
@@ -581,8 +601,10 @@ def run_ours(a):
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": (DOCK_DRAM_BYTES_PER_EVAL[shapes["dock_launch_shape"]] * evals / K
                                  if shapes["dock_launch_shape"] in DOCK_DRAM_BYTES_PER_EVAL else None),
+                     "l1_wavefront_roof": dock_l1_roof(shapes["dock_launch_shape"], evals, dock_ms, clk, local),
                      "note": "algorithmic bytes = evals x (32 x heavy atoms + 16 x intra pairs); traffic = "
-                             "ncu DRAM bytes per evaluation x evaluations per launch"},
+                             "ncu DRAM bytes per evaluation x evaluations per launch; the kernel's limit is the "
+                             "L1 data pipe (l1_wavefront_roof), HBM is a reference point"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk,
