@@ -123,17 +123,39 @@ def lig_bytes(lig):
     return 32 * heavy + 16 * len(lig["pairs"])
 
 
-# DRAM bytes per evaluation of dock_kernel, per launch shape, from ncu
-# captures of this workload (profiles/dock_kernel_wide_box_screen.txt; 4
-# ligands x 6,500 chains, 11.55 M evaluations per launch): 80 registers
-# 5.52 GB per launch.  The bench scales the figure by the evaluations of
-# each launch; shapes not captured report no traffic.
-DOCK_DRAM_BYTES_PER_EVAL = {4: 477.4}
-# L1 data-pipe (LSU) wavefronts per evaluation of dock_kernel, per launch
-# shape, from the same capture (l1tex__data_pipe_lsu_wavefronts.sum over the
-# launch's evaluations): the kernel's limit is that pipe, one wavefront per
-# SM per cycle.  Shapes not captured report no fraction.
-DOCK_L1_WAVEFRONTS_PER_EVAL = {4: 462.7}
+def lig_flops(lig):
+    """Algorithmic FP32 operations of one BFGS evaluation (forward + adjoint):
+    ~115 per heavy atom (trilinear value and gradient ~70, kinematics ~30,
+    adjoint ~15) and ~25 per intra pair."""
+    heavy = int((lig["xs"] >= 0).sum())
+    return 115 * heavy + 25 * len(lig["pairs"])
+
+
+def fp32_roof(flops, ms, clk, device):
+    """Fraction of the FP32 peak (SMs x 128 lanes x 2 flops per FMA x median
+    SM clock) the docking kernel's algorithmic flops reach."""
+    import torch
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = sms * 128 * 2 * mhz * 1e6
+    return {"achieved_tflops": flops / (ms / 1e3) / 1e12, "peak_tflops": peak / 1e12,
+            "frac": flops / (ms / 1e3) / peak, "model": "115 x heavy atoms + 25 x intra pairs per evaluation"}
+
+
+# DRAM bytes and L1 data-pipe (LSU) wavefronts of dock_kernel per
+# algorithmic byte (lig_bytes x evaluations), per launch shape, from a
+# one-pass ncu capture of one full launch of this workload (the first timed
+# batch: 64 ligands x 6,500 chains, 266 M evaluations, 1.91 TB algorithmic;
+# dram__bytes_read.sum + dram__bytes_write.sum = 151.5 GB,
+# l1tex__data_pipe_lsu_wavefronts.sum = 195.2 G; summarised in
+# profiles/dock_kernel_wide_box_screen.txt).  Wavefronts track the
+# algorithmic bytes across ligand sizes (0.1009 per byte on a 4-ligand
+# launch of small ligands, 0.1020 on the full one) where a per-evaluation
+# figure does not (463 vs 733), so the bench scales them by the algorithmic
+# bytes of each timed launch.  The kernel's limit is that pipe, one
+# wavefront per SM per cycle.  Shapes not captured report neither.
+DOCK_DRAM_PER_ABYTE = {4: 0.07919}
+DOCK_L1_WAVEFRONTS_PER_ABYTE = {4: 0.10198}
 DOCK_SHAPES = 3  # launch shapes the docking autotuner explores (register budgets 64 / 80 / 128)
 # L1 data-pipe (LSU) wavefronts of one grid build of this workload (188^3
 # points x 8 maps, 8,000-atom receptor), from the ncu capture summarised in
@@ -158,19 +180,20 @@ def grid_l1_roof(ms, clk, device):
             "frac_of_l1_wavefront_roof": GRID_L1_WAVEFRONTS / (ms / 1e3) / peak}
 
 
-def dock_l1_roof(shape, evals, ms, clk, device):
+def dock_l1_roof(shape, abytes, ms, clk, device):
     """Fraction of the L1 data-pipe wavefront roof the docking kernel
-    reaches over the timed launches: ncu wavefronts per evaluation x the
-    evaluations timed / (kernel time x SMs x median SM clock x 1 wavefront
-    per SM per cycle)."""
-    if shape not in DOCK_L1_WAVEFRONTS_PER_EVAL:
+    reaches over the timed launches: ncu wavefronts per algorithmic byte x
+    the algorithmic bytes timed / (kernel time x SMs x median SM clock x 1
+    wavefront per SM per cycle)."""
+    if shape not in DOCK_L1_WAVEFRONTS_PER_ABYTE:
         return None
     import torch
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     mhz = clk.get("sm_mhz") or 1965.0
-    wf = DOCK_L1_WAVEFRONTS_PER_EVAL[shape] * evals
-    return {"wavefronts_per_eval": DOCK_L1_WAVEFRONTS_PER_EVAL[shape], "wavefronts_per_s": wf / (ms / 1e3),
-            "peak_per_s": sms * mhz * 1e6, "frac": wf / (ms / 1e3) / (sms * mhz * 1e6)}
+    wf = DOCK_L1_WAVEFRONTS_PER_ABYTE[shape] * abytes
+    return {"wavefronts_per_algorithmic_byte": DOCK_L1_WAVEFRONTS_PER_ABYTE[shape],
+            "wavefronts_per_s": wf / (ms / 1e3), "peak_per_s": sms * mhz * 1e6,
+            "frac": wf / (ms / 1e3) / (sms * mhz * 1e6)}
 
 
 def peaks():
@@ -491,7 +514,7 @@ def run_ours(a):
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record()
-    dock_ms, post_ms, evals, abytes, launches = 0.0, 0.0, 0, 0, 0
+    dock_ms, post_ms, evals, abytes, aflops, launches = 0.0, 0.0, 0, 0, 0, 0
     t_wall = time.perf_counter()
     step_wall = []
     for k in range(W, W + K):
@@ -505,6 +528,7 @@ def run_ours(a):
         for lid, r in zip(batches[k], res):
             evals += r["bfgs_evals"]
             abytes += r["bfgs_evals"] * lig_bytes(ligs[lid])
+            aflops += r["bfgs_evals"] * lig_flops(ligs[lid])
         launches += 5  # dock, cluster, gather, refine, score
     ev1.record()
     torch.cuda.synchronize()
@@ -599,12 +623,13 @@ def run_ours(a):
                        **grid_l1_roof(min(grid_ms), clk, local)},
         "roofline": {"kernel": "dock_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": (DOCK_DRAM_BYTES_PER_EVAL[shapes["dock_launch_shape"]] * evals / K
-                                 if shapes["dock_launch_shape"] in DOCK_DRAM_BYTES_PER_EVAL else None),
-                     "l1_wavefront_roof": dock_l1_roof(shapes["dock_launch_shape"], evals, dock_ms, clk, local),
+                     "traffic": (DOCK_DRAM_PER_ABYTE[shapes["dock_launch_shape"]] * abytes / K
+                                 if shapes["dock_launch_shape"] in DOCK_DRAM_PER_ABYTE else None),
+                     "l1_wavefront_roof": dock_l1_roof(shapes["dock_launch_shape"], abytes, dock_ms, clk, local),
+                     "fp32_roof": fp32_roof(aflops, dock_ms, clk, local),
                      "note": "algorithmic bytes = evals x (32 x heavy atoms + 16 x intra pairs); traffic = "
-                             "ncu DRAM bytes per evaluation x evaluations per launch; the kernel's limit is the "
-                             "L1 data pipe (l1_wavefront_roof), HBM is a reference point"},
+                             "ncu DRAM bytes per algorithmic byte x algorithmic bytes per launch; the kernel's "
+                             "limit is the L1 data pipe (l1_wavefront_roof), HBM is a reference point"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk,
