@@ -2,7 +2,8 @@
 config from Vina-CUDA_v1.1/input_file_example): it runs from a --config file,
 writes the reference's multi-MODEL PDBQT with REMARK VINA RESULT lines, and
 its best score lies in the range of the reference's shipped result (-7.9
-kcal/mol, which the README says varies by 0.1-0.5 between runs)."""
+kcal/mol, which the reference's README says varies by 0.1-0.5 between
+runs)."""
 import gzip
 import os
 import subprocess
