@@ -137,7 +137,9 @@ struct SearchMem {  // per-warp shared memory of the optimiser
 
 // quasi_newton.cuh:2172-2389 (RILC-BFGS) with the Lewis-Overton line search
 // of quasi_newton.cuh:1710-1806, on the pose in s.m.x.  Returns the energy;
-// s.m.x holds the optimised pose.  *evals counts energy+gradient calls.
+// s.m.x holds the optimised pose.  *evals counts energy+gradient calls
+// (a trial whose adjoint is skipped counts as one, as the reference's
+// evaluation count does).
 //
 // The loop has one evaluation site: the entry evaluation and every
 // line-search trial run through the same inlined copy of the evaluation
