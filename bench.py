@@ -636,9 +636,10 @@ def run_ours(a):
         "wall_s": t_wall,
     }
     if world == 1 and not a.no_cpu_baseline:
-        # the reference arm's sample of the first two timed steps (the first
-        # cpu_ligands ligands of each batch), after one untimed warm-up ligand
-        sample = [lig for k in range(W, min(W + 2, W + K)) for lig in ligs[k * B:k * B + a.cpu_ligands]]
+        # the first ligand of every timed batch (each also in the reference
+        # arm's sample, which docks the first cpu_ligands of every batch), after
+        # one untimed warm-up ligand: a sample spread over the timed region
+        sample = [ligs[k * B] for k in range(W, W + K)]
         cb = cpu_baseline(xyz, xs, sample, a.chains, len(sample), warm=ligs[0])
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
         line["grid_build"]["cpu_s"] = cb["grid_build_s"]
